@@ -1,0 +1,201 @@
+"""Method data for the H2 maps: what an H2Factory *method* (iFMM, MLFMA, ...) supplies.
+
+H2Factory owns no physics (its docs: docs/src/algorithm.md:34-46): the method provides leaf
+moment collections, level transfers, I2O couplings and near blocks. This module builds them for
+interpolation-based FMMs on a 2^D tree:
+
+* Chebyshev interpolation (black-box FMM): dense or separable transfers, dense M2L blocks per
+  unique translation;
+* equispaced interpolation: identical, but the M2L block of two same-size boxes is multilevel
+  Toeplitz, stored as the FFT of its wrap-around kernel (the H2Toeplitz storage of
+  src/moments/toeplitz/toeplitzmoment.jl:28-30, ext/H2Toeplitz/H2Toeplitz.jl:19-47);
+
+for the Laplace kernel 1/(4 pi |x-y|) and the Helmholtz kernel exp(ik|x-y|)/(4 pi |x-y|), with
+the self term set to zero. Index conventions follow H2Factory's moments: one component array
+of extents (p, p, p) per node, column-major.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .core import H2Core
+from .trees import Tree, build_plans
+
+__all__ = ["laplace", "helmholtz", "chebyshev_nodes", "equispaced_nodes", "lagrange",
+           "interpolation_core", "kernel_matrix"]
+
+
+def laplace(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """1/(4 pi |x - y|) for rows of x against rows of y; zero where x == y."""
+    d = x[:, None, :] - y[None, :, :]
+    r = np.sqrt(np.einsum("ijk,ijk->ij", d, d))
+    with np.errstate(divide="ignore"):
+        k = np.where(r > 0, 1.0 / (4.0 * np.pi * np.where(r > 0, r, 1.0)), 0.0)
+    return k
+
+
+def helmholtz(wavenumber: float):
+    """exp(i k |x - y|)/(4 pi |x - y|); zero where x == y."""
+
+    def kern(x, y):
+        d = x[:, None, :] - y[None, :, :]
+        r = np.sqrt(np.einsum("ijk,ijk->ij", d, d))
+        rs = np.where(r > 0, r, 1.0)
+        return np.where(r > 0, np.exp(1j * wavenumber * rs) / (4.0 * np.pi * rs), 0.0)
+
+    kern.wavenumber = wavenumber
+    return kern
+
+
+def kernel_matrix(kernel, x, y, chunk: int = 2048) -> np.ndarray:
+    """Dense kernel matrix, in row chunks to bound temporaries."""
+    out = None
+    for s in range(0, x.shape[0], chunk):
+        blk = kernel(x[s:s + chunk], y)
+        if out is None:
+            out = np.empty((x.shape[0], y.shape[0]), dtype=blk.dtype)
+        out[s:s + chunk] = blk
+    return out
+
+
+def chebyshev_nodes(p: int) -> np.ndarray:
+    """Chebyshev points of the first kind on [-1, 1]."""
+    k = np.arange(p)
+    return np.cos((2 * k + 1) * np.pi / (2 * p))
+
+
+def equispaced_nodes(p: int) -> np.ndarray:
+    """Cell-centred equispaced points on [-1, 1]: -1 + (2k+1)/p."""
+    return -1.0 + (2.0 * np.arange(p) + 1.0) / p
+
+
+def lagrange(nodes: np.ndarray, t: np.ndarray) -> np.ndarray:
+    """L[k, j] = prod_{m != k} (t_j - xi_m) / (xi_k - xi_m)."""
+    p = nodes.size
+    t = np.asarray(t, dtype=np.float64)
+    L = np.ones((p, t.size))
+    for k in range(p):
+        for m in range(p):
+            if m != k:
+                L[k] *= (t - nodes[m]) / (nodes[k] - nodes[m])
+    return L
+
+
+def _leaf_collection(tree: Tree, leaf: int, nodes: np.ndarray) -> np.ndarray:
+    """(ncoef, nvalues) interpolation matrix of one leaf (column-major coefficient order)."""
+    pts = tree.points[tree.values(leaf)]
+    c, h = tree.center[leaf], tree.halfsize[leaf]
+    p = nodes.size
+    mats = [lagrange(nodes, (pts[:, d] - c[d]) / h) for d in range(tree.dim)]
+    C = mats[0]
+    for d in range(1, tree.dim):
+        # a = a1 + p*a2 + p^2*a3: later axes vary slowest
+        C = (mats[d][:, None, :] * C[None, :, :]).reshape(-1, pts.shape[0])
+    return C
+
+
+def _axis_factors(nodes: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Per-axis child->parent interpolation for the lower (-) and upper (+) child."""
+    lo = lagrange(nodes, -0.5 + 0.5 * nodes)
+    hi = lagrange(nodes, 0.5 + 0.5 * nodes)
+    return lo, hi
+
+
+def _node_grid(tree: Tree, n: int, nodes: np.ndarray) -> np.ndarray:
+    """Interpolation points of box n, ordered like the moment coefficients."""
+    p = nodes.size
+    c, h = tree.center[n], tree.halfsize[n]
+    axes = [c[d] + h * nodes for d in range(tree.dim)]
+    grids = np.meshgrid(*axes, indexing="ij")
+    # column-major flattening: axis 0 fastest
+    return np.stack([g.ravel(order="F") for g in grids], axis=1).reshape(p ** tree.dim, tree.dim)
+
+
+def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
+                       transfers: str = "dense", couplings: str = "dense",
+                       field: str | None = None, precision: str = "fp64",
+                       near: str = "host", alpha=1.0) -> H2Core:
+    """Galerkin H2 core of an interpolation FMM of order `p` on `tree` for `kernel`.
+
+    couplings = "dense" stores one M2L block per unique translation; "toeplitz" stores the
+    FFT'd wrap-around kernel per unique translation (equispaced nodes, same-size boxes only).
+    near = "host" assembles near blocks on the host; "none" leaves them to the caller
+    (e.g. assembled on the device, see h2factory_b200.assembly).
+    """
+    xi = chebyshev_nodes(p) if nodes == "chebyshev" else equispaced_nodes(p)
+    if couplings == "toeplitz" and nodes != "equispaced":
+        raise ValueError("Toeplitz couplings need equispaced interpolation nodes")
+    plans = build_plans(tree)
+    dim = tree.dim
+    cplx = np.iscomplexobj(kernel(np.zeros((1, dim)), np.ones((1, dim))))
+    if field is None:
+        field = "complex" if cplx else "real"
+    dtype = np.complex128 if field == "complex" else np.float64
+    shape = np.zeros((tree.nlevels + 1, 3), np.int32)
+    shape[1:, :] = 1
+    shape[1:, :dim] = p
+
+    leaves = tree.leaves()
+    colls = {int(n): _leaf_collection(tree, int(n), xi).astype(dtype)[None] for n in leaves}
+
+    lo, hi = _axis_factors(xi)
+    tdict = {}
+    for lvl in range(2, tree.nlevels + 1):
+        for s in range(tree.nsectors):
+            facs = [(hi if (s >> d) & 1 else lo).astype(dtype) for d in range(dim)]
+            if transfers == "separable":
+                tdict[(lvl, s)] = tuple(facs)
+            else:
+                T = facs[0]
+                for d in range(1, dim):
+                    T = np.kron(facs[d], T)
+                tdict[(lvl, s)] = T
+
+    far = plans.far
+    ca, cb = tree.center[far[:, 0]], tree.center[far[:, 1]]
+    hmin = np.minimum(tree.halfsize[far[:, 0]], tree.halfsize[far[:, 1]])
+    offs = np.round((cb - ca) / hmin[:, None] * 2).astype(np.int64)
+    keys = np.concatenate([tree.level[far[:, 0]][:, None].astype(np.int64),
+                           tree.level[far[:, 1]][:, None].astype(np.int64), offs], axis=1)
+    ukeys, first, inv = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+    blocks = []
+    for u in range(ukeys.shape[0]):
+        r, t = int(far[first[u], 0]), int(far[first[u], 1])
+        if couplings == "toeplitz":
+            if tree.level[r] != tree.level[t]:
+                raise ValueError("Toeplitz couplings need same-level pairs (uniform trees)")
+            h = tree.halfsize[r]
+            dc = tree.center[r] - tree.center[t]
+            ts = 2 * p - 1
+            m = np.arange(ts)
+            m = np.where(m < p, m, m - ts)          # wrap-around: index mod(i - j, ts)
+            grids = np.meshgrid(*([m] * dim), indexing="ij")
+            z = np.stack([dc[d] + (2.0 * h / p) * grids[d] for d in range(dim)], axis=-1)
+            kv = kernel(z.reshape(-1, dim), np.zeros((1, dim)))[:, 0].reshape((ts,) * dim)
+            blocks.append(np.fft.fftn(kv.astype(np.complex128)))
+        else:
+            B = kernel(_node_grid(tree, r, xi), _node_grid(tree, t, xi)).astype(dtype)
+            blocks.append(B)
+
+    core = H2Core(field=field, test=tree, trial=tree, plans=plans, ncomp=1, dim=dim,
+                  shape_test=shape, shape_trial=shape, collections_test=colls,
+                  collections_trial=colls, transfers_test=tdict, transfers_trial=tdict,
+                  transfer_kind=transfers, coupling_kind=couplings, couplings=blocks,
+                  pair_coupling=inv.reshape(-1).astype(np.int64), precision=precision,
+                  alpha=alpha, conj_leaf_adjoint=(field == "complex"))
+    core.kernel = kernel
+    if near == "host":
+        core.set_near_blocks(near_blocks_from_kernel(tree, plans, kernel, dtype))
+    return core
+
+
+def near_blocks_from_kernel(tree: Tree, plans, kernel, dtype, test: Tree | None = None):
+    """Dense near blocks K(values(a), values(b)) for every near leaf pair, in plan order."""
+    test = tree if test is None else test
+    out = []
+    for a, b in plans.near:
+        xa = test.points[test.values(int(a))]
+        yb = tree.points[tree.values(int(b))]
+        out.append(kernel(xa, yb).astype(dtype))
+    return out

@@ -1,0 +1,232 @@
+/*
+ * h2b200.h -- C ABI of the B200 H2 matrix-vector product.
+ *
+ * The library replaces the execution half of H2Factory.jl's map: the read-only core
+ * (`src/maps/core.jl:17-33`), the per-request workspace (`src/maps/workspace.jl:81-113`) and
+ * `LinearMaps._unsafe_mul!` on it (`src/maps/abstracth2map.jl:42-86`), i.e. near product + far
+ * product (aggregation, I2O, disaggregation) in forward, transpose and adjoint orientation.
+ *
+ * Everything crossing this boundary is plain C: integer index arrays, scalar arrays, sizes,
+ * and opaque handles. Complex scalars are interleaved (re, im) pairs of doubles. Node ids,
+ * degree-of-freedom ids and levels follow H2Trees' conventions restated in a flattened form:
+ *   - node ids are 0-based, levels are 1-based with the root at level 1;
+ *   - a leaf is a node without children;
+ *   - `sector` is H2Trees.sector(tree, child), the 0-based slot of a child in its parent.
+ * Every entry point returns an h2b_status; on failure `h2b_last_error` gives the text.
+ * No C++ exception crosses this boundary.
+ */
+#ifndef H2B200_H
+#define H2B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int h2b_status;
+#define H2B_OK 0
+#define H2B_ERR_INVALID 1     /* malformed descriptor or argument                              */
+#define H2B_ERR_CUDA 2        /* a CUDA runtime call failed                                     */
+#define H2B_ERR_NOMEM 3       /* device allocation failed or the memory budget was exceeded     */
+#define H2B_BUSY 4            /* the workspace is in use (H2Factory's ConcurrentWorkspaceError) */
+#define H2B_ERR_UNSUPPORTED 5 /* valid request this build does not implement                   */
+
+/* Scalar field of x, y, leaf collections, level transfers, couplings and near blocks. */
+#define H2B_REAL 0    /* double                        */
+#define H2B_COMPLEX 1 /* double complex, (re, im) pairs */
+
+/* Arithmetic of the far field (moments, transfers, couplings). The near field and the final
+ * near + far summation always run in the field's FP64 type. */
+#define H2B_FP64 0
+#define H2B_FP32 1
+
+/* Map orientation, H2Factory's isForward / isTranspose / isAdjoint (src/maps/traits.jl:4-8). */
+#define H2B_FORWARD 0
+#define H2B_TRANSPOSE 1
+#define H2B_ADJOINT 2
+
+/* Level-transfer storage, H2Factory's DenseI2I / SeparableI2I (src/maps/leveltranslator.jl:84-118). */
+#define H2B_TRANSFER_DENSE 0
+#define H2B_TRANSFER_SEPARABLE 1
+
+/* I2O coupling storage, H2Factory's DenseTranslation / DiagonalTranslation /
+ * ToeplitzI2OTranslationTrait (src/farinteractions/i2otranslations/i2otranslationtraits.jl:13-41). */
+#define H2B_COUPLING_DENSE 0
+#define H2B_COUPLING_DIAGONAL 1
+#define H2B_COUPLING_TOEPLITZ 2
+
+/*
+ * One tree side (test = rows / y, trial = columns / x) with the plans that use it.
+ *
+ * A side is an aggregation side in one orientation and a disaggregation side in the other:
+ * the trial side aggregates for forward maps and disaggregates for transpose/adjoint maps
+ * (accessors `aggregationplan`/`disaggregationplan`, src/maps/accessors.jl:232-242).
+ */
+typedef struct h2b_side_desc {
+    /* ---- tree (H2Trees.level/parent/sector/children/values) ---- */
+    int32_t nnodes;
+    int32_t nlevels;           /* levels are 1..nlevels */
+    int32_t root;
+    int32_t ndofs;             /* length of x (trial) or y (test)                          */
+    const int32_t *level;      /* [nnodes]                                                  */
+    const int32_t *parent;     /* [nnodes], -1 at the root                                  */
+    const int32_t *sector;     /* [nnodes], 0-based child slot; ignored at the root         */
+    const int32_t *child_ptr;  /* [nnodes+1] CSR of children, in H2Trees.children order    */
+    const int32_t *child;
+    const int32_t *value_ptr;  /* [nnodes+1] CSR of the dofs each leaf owns (empty if inner) */
+    const int32_t *value;      /* 0-based dof ids, H2Trees.values order                     */
+
+    /* ---- moment shape per level (index = level, entries 0 unused) ---- */
+    const int32_t *shape;      /* [(nlevels+1)*3] moment array extents s1,s2,s3 (1 if unused);
+                                  the number of coefficients per component is s1*s2*s3 */
+
+    /* ---- aggregation plan (this side aggregating), levels bottom-up ----
+     * H2Trees.aggregationlevels / aggregationnodes / storenode, as consumed by
+     * aggregatetree! (src/farinteractions/aggregation.jl:58-92, :241-272). */
+    int32_t agg_nstages;
+    const int32_t *agg_level;  /* [agg_nstages] level of each stage, deepest first */
+    const int32_t *agg_ptr;    /* [agg_nstages+1] */
+    const int32_t *agg_node;   /* nodes visited per stage */
+    const uint8_t *agg_store;  /* [nnodes] storenode(plan, node): moment read by I2O */
+
+    /* ---- disaggregation plan (this side receiving), levels top-down ----
+     * H2Trees.isdisaggregationnode / translatingnodes, as consumed by
+     * disaggregatetranslatetree! (src/farinteractions/disaggregation.jl:106-295). */
+    int32_t dis_nstages;
+    const int32_t *dis_level;  /* [dis_nstages] level of each stage, root side first */
+    const int32_t *dis_ptr;    /* [dis_nstages+1] */
+    const int32_t *dis_node;
+    const uint8_t *dis_isnode; /* [nnodes] isdisaggregationnode(plan, node) */
+    const int32_t *i2o_ptr;    /* [nnodes+1] translating partners of each receiving node */
+    const int32_t *i2o_src;    /* partner node ids on the OTHER side */
+    const int64_t *i2o_coupling; /* coupling index of each pair, already resolved through
+                                    couplingkey (src/farinteractions/i2otranslations/i2oprotocol.jl:87-92):
+                                    pair (r, t) on the test side uses the block stored for (r, t);
+                                    on the trial side it uses the block stored for (t, r). */
+
+    /* ---- leaf collections (test/trialmomentcollections) ----
+     * For leaf n: ncomp matrices, each ncoef(level(n)) x nvalues(n), column-major, stored one
+     * after the other from element offset coll_offset[n]. -1 for non-leaves. */
+    const int64_t *coll_offset;  /* [nnodes] */
+    const double *coll;          /* field scalars */
+    int64_t coll_len;            /* in field scalars */
+
+    /* ---- level transfers (this side's I2I translator; O2O applies its transpose/adjoint) ----
+     * transfers[level(child)][sector(child)] (src/maps/leveltranslator.jl:69-72, :110-116).
+     * Dense: one ncoef(level-1) x ncoef(level) column-major matrix.
+     * Separable: `dim` per-axis matrices, axis d being shape[level-1][d] x shape[level][d],
+     * column-major, axis 1 first (src/maps/leveltranslator.jl:168-265). */
+    const int64_t *transfer_offset; /* [(nlevels+1)*nsectors], -1 where absent */
+    const double *transfer;
+    int64_t transfer_len;
+} h2b_side_desc;
+
+/* A complete map (H2Factory's core + the flattened plans that a workspace schedules). */
+typedef struct h2b_map_desc {
+    int32_t field;          /* H2B_REAL / H2B_COMPLEX */
+    int32_t precision;      /* H2B_FP64 / H2B_FP32 far field */
+    int32_t ncomp;          /* moment components D of AbstractMoment{D,T} (abstractmoment.jl:6) */
+    int32_t dim;            /* rank of each moment component array (1..3) */
+    int32_t nsectors;       /* children slots per node, 2^dim for a 2^dim tree */
+    int32_t transfer_kind;  /* H2B_TRANSFER_* */
+    int32_t coupling_kind;  /* H2B_COUPLING_* */
+    int32_t conj_leaf_adjoint; /* leafmul(A, isAdjoint): 1 = ConjugatedCollectionMul,
+                                  0 = LinAlgebraMulFunctor (src/maps/functors.jl:206-259) */
+    double alpha[3][2];     /* α(A, trait) for forward, transpose, adjoint, as (re, im) */
+    h2b_side_desc test;
+    h2b_side_desc trial;
+
+    /* ---- I2O couplings (I2OTranslationCollection values, one per stored block) ----
+     * Dense: ncoef(level r) x ncoef(level t) column-major block for pair (r, t).
+     * Diagonal: ncoef values.
+     * Toeplitz: prod(2s-1) complex values of the FFT'd wrap-around kernel (always complex),
+     *   in column-major order of the padded array (src/moments/toeplitz/toeplitzmoment.jl:28-30). */
+    int64_t ncouplings;
+    const int64_t *coupling_offset; /* [ncouplings] in doubles */
+    const double *coupling;
+    int64_t coupling_len;            /* in doubles */
+
+    /* ---- near field: dense blocks per (test leaf, trial leaf) pair, grouped by test leaf.
+     * Block b is nvalues(row) x nvalues(col), column-major, from element offset near_offset[b];
+     * rows are H2Trees.values(test, row), columns H2Trees.values(trial, col). This is the
+     * BlockSparseMatrix layout of ext/H2BlockSparse/assembly.jl:1-87 for the matrix built by
+     * nearinteractions (src/nearinteractions/nearmul.jl:54-111). */
+    int32_t near_nrows;               /* number of row groups */
+    const int32_t *near_row;          /* [near_nrows] test leaf of each row group */
+    const int32_t *near_ptr;          /* [near_nrows+1] */
+    const int32_t *near_col;          /* trial leaf of each block */
+    const int64_t *near_offset;       /* element offset of each block */
+    const double *near;               /* field scalars; host memory unless near_on_device */
+    int64_t near_len;                 /* in field scalars */
+    int32_t near_on_device;           /* 1: `near` is a device pointer on the core's device */
+} h2b_map_desc;
+
+typedef struct h2b_core h2b_core;
+typedef struct h2b_workspace h2b_workspace;
+
+/* Sizes of a built core, for budgets and reports. */
+typedef struct h2b_core_info {
+    int64_t device_bytes;   /* device memory held by the core */
+    int64_t near_entries;   /* stored near-field scalars */
+    int64_t npairs[2];      /* I2O pairs on the test / trial side */
+    int64_t moment_elems;   /* moment arena elements per right-hand side */
+    int64_t spectrum_elems; /* Toeplitz spectra elements per right-hand side (complex) */
+    int32_t nrows;          /* test dofs  */
+    int32_t ncols;          /* trial dofs */
+} h2b_core_info;
+
+/* Library version, (major << 16) | minor. */
+int32_t h2b_version(void);
+
+/* Text of the last failure on the calling thread. */
+const char *h2b_last_error(void);
+
+/* Validate `desc`, copy it to `device` and build the read-only core: the CUDA equivalent of
+ * building an AbstractH2Core (src/maps/core.jl:17-33). The caller keeps its host arrays. */
+h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **out);
+h2b_status h2b_core_destroy(h2b_core *core);
+h2b_status h2b_core_get_info(const h2b_core *core, h2b_core_info *out);
+
+/* Mutable per-request state (moments, spectra, host staging) for up to `max_nrhs` right-hand
+ * sides: H2Workspace(core) / similarworkspace (src/maps/workspace.jl:81-113). Several
+ * workspaces may share one core. */
+h2b_status h2b_workspace_create(h2b_core *core, int32_t max_nrhs, h2b_workspace **out);
+h2b_status h2b_workspace_destroy(h2b_workspace *ws);
+
+/*
+ * y = α op(A) x + β y on `nrhs` column-major right-hand sides (device pointers, leading
+ * dimensions in scalars), op selected by `mode`; LinearMaps._unsafe_mul! on an H2 map
+ * (src/maps/abstracth2map.jl:42-86): near product with (α, β), then far product with (α, 1).
+ * `alpha`/`beta` point at (re, im) doubles; both NULL gives the 3-argument mul!(y, A, x).
+ * `stream` is a cudaStream_t (NULL = legacy default stream). Asynchronous on `stream`.
+ * A second call on a workspace that is still inside a call returns H2B_BUSY.
+ */
+h2b_status h2b_matvec(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x, int64_t ldx,
+                      void *y, int64_t ldy, const double *alpha, const double *beta,
+                      void *stream);
+
+/* Same product on HOST arrays: copies x in, multiplies, copies y out and synchronizes the
+ * stream before returning. This is the call a host-language binding makes for mul!(y, A, x). */
+h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
+                           int64_t ldx, void *y, int64_t ldy, const double *alpha,
+                           const double *beta, void *stream);
+
+/* Far part only: farmul! (src/farinteractions/farmul.jl:8-70). With alpha = beta = NULL y is
+ * zero-filled first (3-argument form); otherwise only leaves that receive a far contribution
+ * are updated, y_leaf = α α(A) far + β y_leaf. */
+h2b_status h2b_farmul(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x, int64_t ldx,
+                      void *y, int64_t ldy, const double *alpha, const double *beta,
+                      void *stream);
+
+/* Near part only: nearmul! (src/nearinteractions/nearmul.jl:8-14), y = α op(N) x + β y. */
+h2b_status h2b_nearmul(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
+                       int64_t ldx, void *y, int64_t ldy, const double *alpha,
+                       const double *beta, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* H2B200_H */
