@@ -1,0 +1,428 @@
+"""Benchmark of the B200 H2 matvec on the Toeplitz far-field workload.
+
+Workload (synthetic, seeded): Laplace kernel 1/(4 pi |x-y|), N = 262144 points uniform in the unit
+cube, uniform octree of depth 5 (4096 leaves, ~64 points per leaf), equispaced interpolation p = 4
+per axis with Toeplitz M2L (FFT on (2p-1)^3 = 7^3 padded grids), dense FP64 near blocks of adjacent
+leaves (97,336 blocks, ~399 M entries). One step = one matvec on one right-hand-side block,
+alternating forward and transpose. The near blocks (3.2 GB) exceed L2 (126 MB), so no L2 flush is
+needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--form plain|chosen]
+
+Rank 0 prints one JSON line. With N > 1 every rank runs an independent replica of the map (the
+single-map product does not shard), timing is the max over ranks, and `value` is the total
+right-hand sides of all ranks per second.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "h2factory.jl_b200")
+METRIC = "H2 matvec RHS/s + p50/p99 latency at <=1e-6 rel err vs FP64; served vs plain"
+WORKLOAD = "toeplitz-laplace-N262144-depth5-p4"
+
+
+def _package():
+    if "h2factory_b200" in sys.modules:
+        return sys.modules["h2factory_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "h2factory_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["h2factory_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Per-launch DRAM bytes of kernels captured with ncu (profiles/ncu_traffic.txt)."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if os.path.exists(path):
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#"):
+                out[(parts[0], parts[1])] = float(parts[2])
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------------------------
+def build_core(n=262144, depth=5, p=4, seed=0, device="cuda:0", precision="fp64"):
+    h2 = _package()
+    from h2factory_b200 import assembly, methods, trees
+
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n, 3))
+    pts = pts[trees.morton_order(pts)]
+    tree = trees.build_tree(pts, depth=depth, root_center=[0.5] * 3, root_halfsize=0.5)
+    core = methods.interpolation_core(tree, methods.laplace, p, nodes="equispaced",
+                                      couplings="toeplitz", transfers="dense", near="none",
+                                      precision=precision)
+    assembly.near_blocks_device(core, "laplace", device=device)
+    return h2, core
+
+
+def launches_per_step(core, mode: int) -> int:
+    """Kernels one h2b_matvec enqueues (same node-list logic as the library)."""
+    agg = core.plans.trial if mode == 0 else core.plans.test
+    dis = core.plans.test if mode == 0 else core.plans.trial
+    tree = core.trial if mode == 0 else core.test
+    dtree = core.test if mode == 0 else core.trial
+    count = 1  # near
+    count += 1  # leaf aggregation
+    for st in range(agg.agg_level.size):
+        nodes = agg.agg_node[agg.agg_ptr[st]:agg.agg_ptr[st + 1]]
+        if any(not tree.isleaf(int(n)) for n in nodes):
+            count += 1
+    toep = core.coupling_kind == "toeplitz"
+    count += 1 + (2 if toep else 0)  # i2o (+ fft in / out)
+    for st in range(dis.dis_level.size):
+        nodes = dis.dis_node[dis.dis_ptr[st]:dis.dis_ptr[st + 1]]
+        if any(int(n) != 0 and dis.dis_isnode[dtree.parent[int(n)]] for n in nodes):
+            count += 1
+    count += 1  # leaf disaggregation
+    return count
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def time_loop(torch, fn, steps, warmup, stream):
+    """Per-step device times (ms) from CUDA events on `stream`, and the total."""
+    for i in range(warmup):
+        fn(i)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for i in range(steps):
+            fn(i)
+            ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+    return per, ev[0].elapsed_time(ev[steps])
+
+
+def pct(v, q):
+    return float(np.percentile(np.asarray(v), q))
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU arms
+# ---------------------------------------------------------------------------------------------
+def cpu_matvec_rate(core, seconds=15.0, nthreads=0):
+    """The oracle (a CPU port of the reference algorithm) on the host cores: RHS/s over a bounded
+    number of forward/transpose matvecs of the full workload."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    from h2factory_b200.core import flatten
+
+    desc = flatten(core)
+    threads = nthreads or oracle.max_threads()
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(core.trial.npoints)
+    oracle.matvec(core, x, 0, nthreads=threads, desc=desc)  # warm
+    done, t0, times = 0, time.perf_counter(), []
+    while time.perf_counter() - t0 < seconds or done < 2:
+        t1 = time.perf_counter()
+        oracle.matvec(core, x, done % 2, nthreads=threads, desc=desc)
+        times.append(time.perf_counter() - t1)
+        done += 1
+    wall = time.perf_counter() - t0
+    return {"value": done / wall, "unit": "RHS/s", "cores": threads, "kind": "port",
+            "sample": f"{done} full matvecs (alternating forward/transpose, 1 RHS) in {wall:.1f} s",
+            "p50_ms": pct(times, 50) * 1e3, "p99_ms": pct(times, 99) * 1e3}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    import torch
+
+    device = "cuda:0" if torch.cuda.is_available() else "cpu"
+    if device == "cpu":
+        h2, core = build_core_cpu()
+    else:
+        h2, core = build_core(device=device)
+        core.near_data = core.near_device.cpu().numpy()
+        core.near_device = None
+        torch.cuda.empty_cache()
+    per = max(1, args.steps)
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    from h2factory_b200.core import flatten
+
+    desc = flatten(core)
+    threads = oracle.max_threads()
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(core.trial.npoints)
+    for i in range(args.warmup):
+        oracle.matvec(core, x, i % 2, nthreads=threads, desc=desc)
+    times = []
+    for i in range(per):
+        t1 = time.perf_counter()
+        oracle.matvec(core, x, i % 2, nthreads=threads, desc=desc)
+        times.append(time.perf_counter() - t1)
+    tot = sum(times)
+    value = per / tot
+    line = {"metric": METRIC, "value": value, "unit": "RHS/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": per, "warmup": args.warmup, "ms_per_step": tot / per * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "rhs_per_step": 1, "modes": "forward/transpose alternating"},
+            "p50_ms": pct(times, 50) * 1e3, "p99_ms": pct(times, 99) * 1e3,
+            "cpu_baseline": {"value": value, "unit": "RHS/s", "cores": threads, "kind": "port",
+                             "sample": f"{per} full matvecs of the workload after {args.warmup} warm-up"},
+            "e2e": {"value": value, "unit": "RHS/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference is Julia and cannot run here; this arm times the C restatement of its "
+                    "CPU algorithm (oracle/) with OpenMP over node chunks"}
+    print(json.dumps(line), flush=True)
+
+
+def build_core_cpu():
+    h2 = _package()
+    from h2factory_b200 import methods, trees
+
+    rng = np.random.default_rng(0)
+    pts = rng.random((262144, 3))
+    pts = pts[trees.morton_order(pts)]
+    tree = trees.build_tree(pts, depth=5, root_center=[0.5] * 3, root_halfsize=0.5)
+    core = methods.interpolation_core(tree, methods.laplace, 4, nodes="equispaced", couplings="toeplitz")
+    return h2, core
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    device = f"cuda:{local_rank}"
+    h2, core = build_core(device=device, precision="fp64")
+    nrhs = args.nrhs
+    ws = h2.H2Workspace(core, max_nrhs=nrhs, device=local_rank)
+    n = core.trial.npoints
+    rng = np.random.default_rng(100 + rank)
+    xh = rng.standard_normal((n, nrhs))
+    x = torch.from_numpy(np.ascontiguousarray(xh.T)).to(device).t()
+    ys = [torch.zeros((nrhs, n), dtype=torch.float64, device=device).t() for _ in range(2)]
+    views = [ws, h2.transpose(ws)]
+    stream = torch.cuda.current_stream(device)
+    sptr = stream.cuda_stream
+
+    def step(i):
+        h2.mul_(ys[i % 2], views[i % 2], x, stream=sptr)
+
+    # accuracy of this form against the CPU oracle (rank 0, before timing)
+    acc = {}
+    if rank == 0 and not args.skip_check:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle
+
+        host_core = core
+        near_host = core.near_device.cpu().numpy()
+        saved = (core.near_device, core.near_data)
+        core.near_data, core.near_device = near_host, None
+        want = oracle.matvec(host_core, xh[:, 0], 0)
+        core.near_device, core.near_data = saved
+        y0 = torch.zeros(n, dtype=torch.float64, device=device)
+        h2.mul_(y0, ws, x[:, 0].contiguous())
+        got = y0.cpu().numpy()
+        acc["rel_err_vs_fp64_oracle"] = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+        # method error against the dense kernel on 512 sampled rows (FP64 direct sums)
+        rows = rng.choice(n, 512, replace=False)
+        P = torch.from_numpy(core.test.points).to(device)
+        d = P[torch.from_numpy(rows).to(device)][:, None, :] - P[None, :, :]
+        r = torch.sqrt((d * d).sum(-1))
+        K = torch.where(r > 0, 1.0 / (4 * np.pi * torch.where(r > 0, r, torch.ones_like(r))), torch.zeros_like(r))
+        exact = (K @ x[:, 0].contiguous()).cpu().numpy()
+        acc["method_rel_err_vs_dense_512rows"] = float(np.linalg.norm(got[rows] - exact) / np.linalg.norm(exact))
+        del d, r, K
+        torch.cuda.empty_cache()
+        cpu = cpu_matvec_rate(core_with_host_near(core, near_host), seconds=args.cpu_seconds)
+        del near_host
+    if world > 1:
+        torch.distributed.barrier()
+
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        per, total = time_loop(torch, step, args.steps, args.warmup, stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        # dominant kernel: near field, timed alone on the same stream
+        yn = ys[0]
+        nper, ntotal = time_loop(torch, lambda i: h2.nearmul_(yn, ws, x, stream=sptr),
+                                 max(args.steps, 5), 3, stream)
+    tmax = total
+    if world > 1:
+        t = torch.tensor([total], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tmax = float(t.item())
+
+    # end to end through the host-buffer C-ABI call (pinned host memory, copies inside)
+    xpin = torch.from_numpy(np.asfortranarray(xh)).pin_memory().numpy()
+    ypin = torch.zeros((nrhs, n), dtype=torch.float64).pin_memory().numpy().T
+    for i in range(2):
+        ws.matvec_host(xpin, i % 2, y=ypin)
+    te = []
+    for i in range(args.steps):
+        t1 = time.perf_counter()
+        ws.matvec_host(xpin, i % 2, y=ypin)
+        te.append(time.perf_counter() - t1)
+    e2e_total = sum(te)
+
+    if rank != 0:
+        return
+    hbm, peak_kind = peaks()
+    info = ws.dcore.info()
+    near_bytes = info.near_entries * 8 + 2 * n * 8 * nrhs
+    near_ms = ntotal / len(nper)
+    achieved = near_bytes / (near_ms * 1e-3) / 1e9
+    traffic = traffic_table().get(("near_forward_kernel", WORKLOAD))
+    launches = sum(launches_per_step(core, i % 2) for i in range(args.steps))
+    rhs_total = args.steps * nrhs * world
+    line = {
+        "metric": METRIC, "value": rhs_total / (tmax * 1e-3), "unit": "RHS/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tmax / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded uniform points in the unit cube)",
+        "config": {"workload": WORKLOAD, "form": "plain (FP64 far and near)", "rhs_per_step": nrhs,
+                   "modes": "forward/transpose alternating", "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (3.2 GB near blocks); no flush",
+                   "near_entries": int(info.near_entries), "i2o_pairs": int(info.npairs[0])},
+        "p50_ms": pct(per, 50), "p99_ms": pct(per, 99),
+        "accuracy": acc,
+        "e2e": {"value": rhs_total / world / e2e_total, "unit": "RHS/s",
+                "h2d_bytes_per_step": int(n * 8 * nrhs), "d2h_bytes_per_step": int(n * 8 * nrhs),
+                "p50_ms": pct(te, 50) * 1e3, "p99_ms": pct(te, 99) * 1e3},
+        "roofline": {"kernel": "near_forward_kernel", "bound": "hbm", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes": near_bytes, "avg_launch_ms": near_ms},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+    }
+    if not args.skip_check:
+        line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line), flush=True)
+
+
+def core_with_host_near(core, near_host):
+    import copy
+
+    c = copy.copy(core)
+    c.near_data, c.near_device = near_host, None
+    return c
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nrhs", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--skip-check", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        gpu_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,882 @@
+// C ABI of the B200 H2 matvec: core upload and validation, workspaces, and the orchestration of
+// the near and far passes (LinearMaps._unsafe_mul! on an H2 map, src/maps/abstracth2map.jl:42-86).
+//
+// Every index array of the descriptor is validated on the host before anything reaches the GPU,
+// so no kernel can be handed an out-of-range node, dof, coupling or block offset.
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "h2b_internal.cuh"
+
+using namespace h2b;
+
+namespace {
+
+thread_local std::string g_err;
+
+h2b_status fail(h2b_status st, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return st;
+}
+
+#define CUDA_TRY(expr)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (expr);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(e_ == cudaErrorMemoryAllocation ? H2B_ERR_NOMEM : H2B_ERR_CUDA,        \
+                        "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+struct Stage {
+    int level = 0;
+    int n = 0;
+    int *d_nodes = nullptr;
+};
+
+struct SideHost {
+    int nnodes = 0, nlevels = 0, ndofs = 0;
+    std::vector<int> level, shape;
+    int maxcoef = 1, maxtsize = 1, maxvals = 1;
+    int maxsep = 1;  // bound on separable-contraction intermediates between adjacent levels
+    int64_t mom_total = 0, spec_total = 0;  // per unit right-hand side
+    int *d_agg_leaves = nullptr;
+    int n_agg_leaves = 0;
+    std::vector<Stage> agg_inner;           // bottom-up
+    int *d_store = nullptr;
+    int n_store = 0;
+    int *d_recv = nullptr;
+    int n_recv = 0;
+    std::vector<Stage> dis_down;            // top-down, nodes with a disaggregation parent
+    uint8_t *d_received = nullptr;
+    int *d_init_leaves = nullptr;
+    int n_init_leaves = 0;
+    int64_t npairs = 0;
+    DSide d{};
+};
+
+}  // namespace
+
+struct h2b_core {
+    int device = 0;
+    int field = H2B_REAL, precision = H2B_FP64;
+    bool conj_leaf = false;
+    cdouble alpha[3];
+    DMap dmap{};
+    DNear dnear{};
+    SideHost test, trial;
+    int near_maxvals = 1;
+    int64_t near_entries = 0;
+    std::vector<void *> allocs;
+    int64_t bytes = 0;
+
+    template <class X>
+    cudaError_t alloc(X **p, size_t count) {
+        *p = nullptr;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)p, count * sizeof(X));
+        if (e == cudaSuccess) {
+            allocs.push_back((void *)*p);
+            bytes += (int64_t)(count * sizeof(X));
+        }
+        return e;
+    }
+    template <class X>
+    cudaError_t upload(X **p, const X *src, size_t count) {
+        cudaError_t e = alloc(p, count);
+        if (e != cudaSuccess || count == 0) return e;
+        return cudaMemcpy(*p, src, count * sizeof(X), cudaMemcpyHostToDevice);
+    }
+    void release() {
+        for (void *p : allocs) cudaFree(p);
+        allocs.clear();
+    }
+};
+
+struct h2b_workspace {
+    h2b_core *core = nullptr;
+    int max_nrhs = 1;
+    void *am = nullptr, *dm = nullptr, *as = nullptr, *ds = nullptr;
+    void *xbuf = nullptr, *ybuf = nullptr;  // staging for h2b_matvec_host
+    std::atomic<int> busy{0};
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// Descriptor validation
+// ---------------------------------------------------------------------------------------------
+int64_t ncoef_host(const h2b_side_desc &s, int lvl) {
+    return (int64_t)s.shape[3 * lvl] * s.shape[3 * lvl + 1] * s.shape[3 * lvl + 2];
+}
+int64_t tsize_host(const h2b_side_desc &s, int lvl) {
+    return (2 * (int64_t)s.shape[3 * lvl] - 1) * (2 * (int64_t)s.shape[3 * lvl + 1] - 1) *
+           (2 * (int64_t)s.shape[3 * lvl + 2] - 1);
+}
+bool isleaf(const h2b_side_desc &s, int n) { return s.child_ptr[n + 1] == s.child_ptr[n]; }
+
+h2b_status validate_side(const h2b_map_desc &d, const h2b_side_desc &s, const h2b_side_desc &other,
+                         const char *name) {
+    if (s.nnodes < 1 || s.nlevels < 1 || s.ndofs < 0)
+        return fail(H2B_ERR_INVALID, "%s: nnodes/nlevels must be positive", name);
+    if (!s.level || !s.parent || !s.sector || !s.child_ptr || !s.value_ptr || !s.shape ||
+        !s.agg_ptr || !s.dis_ptr || !s.agg_store || !s.dis_isnode || !s.i2o_ptr || !s.coll_offset ||
+        !s.transfer_offset)
+        return fail(H2B_ERR_INVALID, "%s: missing array", name);
+    if (s.root < 0 || s.root >= s.nnodes || s.parent[s.root] != -1)
+        return fail(H2B_ERR_INVALID, "%s: bad root", name);
+    for (int l = 1; l <= s.nlevels; ++l) {
+        for (int k = 0; k < 3; ++k)
+            if (s.shape[3 * l + k] < 1 || s.shape[3 * l + k] > 64)
+                return fail(H2B_ERR_INVALID, "%s: moment extent out of range at level %d", name, l);
+        if (ncoef_host(s, l) > 4096)
+            return fail(H2B_ERR_UNSUPPORTED, "%s: more than 4096 coefficients at level %d", name, l);
+        for (int k = d.dim; k < 3; ++k)
+            if (s.shape[3 * l + k] != 1)
+                return fail(H2B_ERR_INVALID, "%s: extent of unused axis %d must be 1", name, k + 1);
+    }
+    if (s.child_ptr[0] != 0) return fail(H2B_ERR_INVALID, "%s: child_ptr[0] != 0", name);
+    if (s.value_ptr[0] != 0) return fail(H2B_ERR_INVALID, "%s: value_ptr[0] != 0", name);
+    for (int n = 0; n < s.nnodes; ++n) {
+        if (s.level[n] < 1 || s.level[n] > s.nlevels) return fail(H2B_ERR_INVALID, "%s: level of node %d", name, n);
+        if (s.child_ptr[n + 1] < s.child_ptr[n]) return fail(H2B_ERR_INVALID, "%s: child_ptr not monotone", name);
+        if (s.value_ptr[n + 1] < s.value_ptr[n]) return fail(H2B_ERR_INVALID, "%s: value_ptr not monotone", name);
+        if (n != s.root) {
+            const int p = s.parent[n];
+            if (p < 0 || p >= s.nnodes) return fail(H2B_ERR_INVALID, "%s: parent of node %d", name, n);
+            if (s.level[n] != s.level[p] + 1) return fail(H2B_ERR_INVALID, "%s: level of node %d vs parent", name, n);
+            if (s.sector[n] < 0 || s.sector[n] >= d.nsectors)
+                return fail(H2B_ERR_INVALID, "%s: sector of node %d", name, n);
+        }
+        if (!isleaf(s, n) && s.value_ptr[n + 1] != s.value_ptr[n])
+            return fail(H2B_ERR_INVALID, "%s: inner node %d owns values", name, n);
+    }
+    const int nch = s.child_ptr[s.nnodes];
+    if (nch > 0 && !s.child) return fail(H2B_ERR_INVALID, "%s: missing children", name);
+    for (int n = 0; n < s.nnodes; ++n)
+        for (int k = s.child_ptr[n]; k < s.child_ptr[n + 1]; ++k) {
+            const int c = s.child[k];
+            if (c < 0 || c >= s.nnodes || s.parent[c] != n)
+                return fail(H2B_ERR_INVALID, "%s: child %d of node %d", name, c, n);
+        }
+    const int nval = s.value_ptr[s.nnodes];
+    if (nval > 0 && !s.value) return fail(H2B_ERR_INVALID, "%s: missing values", name);
+    for (int k = 0; k < nval; ++k)
+        if (s.value[k] < 0 || s.value[k] >= s.ndofs) return fail(H2B_ERR_INVALID, "%s: dof id out of range", name);
+
+    // aggregation plan
+    std::vector<uint8_t> inagg(s.nnodes, 0);
+    if (s.agg_nstages < 0 || s.agg_ptr[0] != 0) return fail(H2B_ERR_INVALID, "%s: agg_ptr", name);
+    for (int st = 0; st < s.agg_nstages; ++st) {
+        if (s.agg_ptr[st + 1] < s.agg_ptr[st]) return fail(H2B_ERR_INVALID, "%s: agg_ptr not monotone", name);
+        if (st > 0 && s.agg_level[st] >= s.agg_level[st - 1])
+            return fail(H2B_ERR_INVALID, "%s: aggregation stages must go bottom-up", name);
+        for (int k = s.agg_ptr[st]; k < s.agg_ptr[st + 1]; ++k) {
+            const int n = s.agg_node[k];
+            if (n < 0 || n >= s.nnodes || s.level[n] != s.agg_level[st])
+                return fail(H2B_ERR_INVALID, "%s: aggregation node %d", name, n);
+            if (inagg[n]) return fail(H2B_ERR_INVALID, "%s: aggregation node %d listed twice", name, n);
+            for (int q = s.child_ptr[n]; q < s.child_ptr[n + 1]; ++q)
+                if (!inagg[s.child[q]])
+                    return fail(H2B_ERR_INVALID, "%s: child %d of aggregation node %d is not aggregated first",
+                                name, s.child[q], n);
+            inagg[n] = 1;
+        }
+    }
+    // disaggregation plan
+    std::vector<uint8_t> indis(s.nnodes, 0);
+    if (s.dis_nstages < 0 || s.dis_ptr[0] != 0) return fail(H2B_ERR_INVALID, "%s: dis_ptr", name);
+    if (s.i2o_ptr[0] != 0) return fail(H2B_ERR_INVALID, "%s: i2o_ptr[0] != 0", name);
+    for (int n = 0; n < s.nnodes; ++n)
+        if (s.i2o_ptr[n + 1] < s.i2o_ptr[n]) return fail(H2B_ERR_INVALID, "%s: i2o_ptr not monotone", name);
+    for (int st = 0; st < s.dis_nstages; ++st) {
+        if (s.dis_ptr[st + 1] < s.dis_ptr[st]) return fail(H2B_ERR_INVALID, "%s: dis_ptr not monotone", name);
+        if (st > 0 && s.dis_level[st] <= s.dis_level[st - 1])
+            return fail(H2B_ERR_INVALID, "%s: disaggregation stages must go top-down", name);
+        for (int k = s.dis_ptr[st]; k < s.dis_ptr[st + 1]; ++k) {
+            const int n = s.dis_node[k];
+            if (n < 0 || n >= s.nnodes || s.level[n] != s.dis_level[st] || !s.dis_isnode[n])
+                return fail(H2B_ERR_INVALID, "%s: disaggregation node %d", name, n);
+            if (indis[n]) return fail(H2B_ERR_INVALID, "%s: disaggregation node %d listed twice", name, n);
+            const bool recv = s.i2o_ptr[n + 1] > s.i2o_ptr[n];
+            const bool fromparent = n != s.root && s.dis_isnode[s.parent[n]];
+            if (fromparent && !indis[s.parent[n]])
+                return fail(H2B_ERR_INVALID, "%s: parent of %d is disaggregated later", name, n);
+            if (!recv && !fromparent)
+                return fail(H2B_ERR_INVALID, "%s: disaggregation node %d receives nothing", name, n);
+            indis[n] = 1;
+        }
+    }
+    for (int n = 0; n < s.nnodes; ++n) {
+        if (s.dis_isnode[n] && !indis[n]) return fail(H2B_ERR_INVALID, "%s: node %d flagged but not scheduled", name, n);
+        if (s.i2o_ptr[n + 1] > s.i2o_ptr[n] && !indis[n])
+            return fail(H2B_ERR_INVALID, "%s: receiving node %d is not a disaggregation node", name, n);
+    }
+    const int npairs = s.i2o_ptr[s.nnodes];
+    if (npairs > 0 && (!s.i2o_src || !s.i2o_coupling)) return fail(H2B_ERR_INVALID, "%s: missing pairs", name);
+    for (int n = 0; n < s.nnodes; ++n)
+        for (int p = s.i2o_ptr[n]; p < s.i2o_ptr[n + 1]; ++p) {
+            const int src = s.i2o_src[p];
+            if (src < 0 || src >= other.nnodes) return fail(H2B_ERR_INVALID, "%s: pair source out of range", name);
+            if (!other.agg_store[src])
+                return fail(H2B_ERR_INVALID, "%s: pair source %d is not a stored aggregation node", name, src);
+            const int64_t key = s.i2o_coupling[p];
+            if (key < 0 || key >= d.ncouplings) return fail(H2B_ERR_INVALID, "%s: coupling index out of range", name);
+            const int64_t off = d.coupling_offset[key];
+            int64_t need;
+            const int64_t nr = ncoef_host(s, s.level[n]), nt = ncoef_host(other, other.level[src]);
+            const int fw = d.field == H2B_COMPLEX ? 2 : 1;
+            if (d.coupling_kind == H2B_COUPLING_DENSE) need = nr * nt * fw;
+            else if (d.coupling_kind == H2B_COUPLING_DIAGONAL) {
+                if (nr != nt) return fail(H2B_ERR_INVALID, "%s: diagonal coupling between different sizes", name);
+                need = nr * fw;
+            } else {
+                for (int k = 0; k < 3; ++k)
+                    if (s.shape[3 * s.level[n] + k] != other.shape[3 * other.level[src] + k])
+                        return fail(H2B_ERR_INVALID, "%s: Toeplitz pair with different moment shapes", name);
+                need = tsize_host(s, s.level[n]) * 2;
+            }
+            if (off < 0 || off + need > d.coupling_len)
+                return fail(H2B_ERR_INVALID, "%s: coupling %lld exceeds the coupling array", name, (long long)key);
+        }
+    // leaf collections of every leaf either plan touches
+    const int fw = d.field == H2B_COMPLEX ? 2 : 1;
+    (void)fw;
+    for (int n = 0; n < s.nnodes; ++n) {
+        if (!isleaf(s, n) || (!inagg[n] && !indis[n])) continue;
+        const int64_t nv = s.value_ptr[n + 1] - s.value_ptr[n];
+        const int64_t off = s.coll_offset[n];
+        if (off < 0 || off + d.ncomp * ncoef_host(s, s.level[n]) * nv > s.coll_len)
+            return fail(H2B_ERR_INVALID, "%s: leaf collection of node %d out of range", name, n);
+    }
+    // transfers of every edge either plan uses
+    for (int n = 0; n < s.nnodes; ++n) {
+        if (n == s.root) continue;
+        const int p = s.parent[n];
+        const bool used = (inagg[p] && inagg[n]) || (indis[n] && s.dis_isnode[p]);
+        if (!used) continue;
+        const int64_t off = s.transfer_offset[(int64_t)s.level[n] * d.nsectors + s.sector[n]];
+        int64_t need;
+        if (d.transfer_kind == H2B_TRANSFER_DENSE) need = ncoef_host(s, s.level[p]) * ncoef_host(s, s.level[n]);
+        else {
+            need = 0;
+            for (int k = 0; k < d.dim; ++k)
+                need += (int64_t)s.shape[3 * s.level[p] + k] * s.shape[3 * s.level[n] + k];
+        }
+        if (off < 0 || off + need > s.transfer_len)
+            return fail(H2B_ERR_INVALID, "%s: transfer (level %d, sector %d) missing", name, s.level[n], s.sector[n]);
+    }
+    return H2B_OK;
+}
+
+h2b_status validate(const h2b_map_desc &d) {
+    if (d.field != H2B_REAL && d.field != H2B_COMPLEX) return fail(H2B_ERR_INVALID, "field must be H2B_REAL or H2B_COMPLEX");
+    if (d.precision != H2B_FP64 && d.precision != H2B_FP32) return fail(H2B_ERR_INVALID, "precision must be H2B_FP64 or H2B_FP32");
+    if (d.ncomp < 1 || d.ncomp > 16) return fail(H2B_ERR_INVALID, "ncomp must be 1..16");
+    if (d.dim < 1 || d.dim > 3) return fail(H2B_ERR_INVALID, "dim must be 1..3");
+    if (d.nsectors < 1 || d.nsectors > 64) return fail(H2B_ERR_INVALID, "nsectors must be 1..64");
+    if (d.transfer_kind != H2B_TRANSFER_DENSE && d.transfer_kind != H2B_TRANSFER_SEPARABLE)
+        return fail(H2B_ERR_INVALID, "unknown transfer kind");
+    if (d.coupling_kind < H2B_COUPLING_DENSE || d.coupling_kind > H2B_COUPLING_TOEPLITZ)
+        return fail(H2B_ERR_INVALID, "unknown coupling kind");
+    if (d.ncouplings < 0 || (d.ncouplings > 0 && (!d.coupling_offset || !d.coupling)))
+        return fail(H2B_ERR_INVALID, "coupling arrays");
+    if (d.field == H2B_REAL)
+        for (int m = 0; m < 3; ++m)
+            if (d.alpha[m][1] != 0.0) return fail(H2B_ERR_INVALID, "complex alpha on a real map");
+    for (const h2b_side_desc *s : {&d.test, &d.trial}) {
+        if (!s->agg_store || s->nnodes < 1) return fail(H2B_ERR_INVALID, "side without nodes or agg_store");
+        if ((s->coll_len > 0 && !s->coll) || (s->transfer_len > 0 && !s->transfer) || s->coll_len < 0 ||
+            s->transfer_len < 0)
+            return fail(H2B_ERR_INVALID, "collection/transfer array missing");
+    }
+    if (d.coupling_len < 0 || (d.coupling_len > 0 && !d.coupling)) return fail(H2B_ERR_INVALID, "coupling array missing");
+    if (d.near_len < 0 || (d.near_len > 0 && !d.near)) return fail(H2B_ERR_INVALID, "near array missing");
+    h2b_status st = validate_side(d, d.test, d.trial, "test");
+    if (st) return st;
+    st = validate_side(d, d.trial, d.test, "trial");
+    if (st) return st;
+    if (d.coupling_kind == H2B_COUPLING_TOEPLITZ) {
+        for (const h2b_side_desc *s : {&d.test, &d.trial})
+            for (int l = 1; l <= s->nlevels; ++l)
+                if (tsize_host(*s, l) > 4096)
+                    return fail(H2B_ERR_UNSUPPORTED, "Toeplitz padded arrays above 4096 entries");
+    }
+    // near blocks
+    if (d.near_nrows < 0) return fail(H2B_ERR_INVALID, "near_nrows");
+    if (d.near_nrows > 0 && (!d.near_row || !d.near_ptr || !d.near_offset || !d.near))
+        return fail(H2B_ERR_INVALID, "near arrays");
+    if (d.near_nrows > 0 && d.near_ptr[0] != 0) return fail(H2B_ERR_INVALID, "near_ptr[0] != 0");
+    for (int g = 0; g < d.near_nrows; ++g) {
+        const int row = d.near_row[g];
+        if (row < 0 || row >= d.test.nnodes || !isleaf(d.test, row))
+            return fail(H2B_ERR_INVALID, "near row group %d is not a test leaf", g);
+        if (d.near_ptr[g + 1] < d.near_ptr[g]) return fail(H2B_ERR_INVALID, "near_ptr not monotone");
+        const int64_t nr = d.test.value_ptr[row + 1] - d.test.value_ptr[row];
+        for (int b = d.near_ptr[g]; b < d.near_ptr[g + 1]; ++b) {
+            const int col = d.near_col[b];
+            if (col < 0 || col >= d.trial.nnodes || !isleaf(d.trial, col))
+                return fail(H2B_ERR_INVALID, "near block %d: column is not a trial leaf", b);
+            const int64_t nc = d.trial.value_ptr[col + 1] - d.trial.value_ptr[col];
+            if (d.near_offset[b] < 0 || d.near_offset[b] + nr * nc > d.near_len)
+                return fail(H2B_ERR_INVALID, "near block %d exceeds the near array", b);
+        }
+    }
+    return H2B_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Upload
+// ---------------------------------------------------------------------------------------------
+template <class T>
+void convert_scalars(const double *src, int64_t count_scalars, bool cplx, std::vector<T> &out);
+
+template <>
+void convert_scalars<double>(const double *src, int64_t n, bool, std::vector<double> &out) {
+    out.assign(src, src + n);
+}
+template <>
+void convert_scalars<float>(const double *src, int64_t n, bool, std::vector<float> &out) {
+    out.resize(n);
+    for (int64_t i = 0; i < n; ++i) out[i] = (float)src[i];
+}
+template <>
+void convert_scalars<cdouble>(const double *src, int64_t n, bool, std::vector<cdouble> &out) {
+    out.resize(n);
+    for (int64_t i = 0; i < n; ++i) out[i] = {src[2 * i], src[2 * i + 1]};
+}
+template <>
+void convert_scalars<cfloat>(const double *src, int64_t n, bool, std::vector<cfloat> &out) {
+    out.resize(n);
+    for (int64_t i = 0; i < n; ++i) out[i] = {(float)src[2 * i], (float)src[2 * i + 1]};
+}
+
+template <class T>
+h2b_status upload_scalars(h2b_core *c, const double *src, int64_t count, const void **dst) {
+    std::vector<T> tmp;
+    convert_scalars<T>(src, count, ScalarTraits<T>::is_complex, tmp);
+    T *p = nullptr;
+    CUDA_TRY(c->upload(&p, tmp.data(), tmp.size()));
+    *dst = p;
+    return H2B_OK;
+}
+
+h2b_status upload_far_scalars(h2b_core *c, const double *src, int64_t count, const void **dst) {
+    const bool cplx = c->field == H2B_COMPLEX;
+    if (!cplx && c->precision == H2B_FP64) return upload_scalars<double>(c, src, count, dst);
+    if (!cplx) return upload_scalars<float>(c, src, count, dst);
+    if (c->precision == H2B_FP64) return upload_scalars<cdouble>(c, src, count, dst);
+    return upload_scalars<cfloat>(c, src, count, dst);
+}
+
+h2b_status upload_list(h2b_core *c, const std::vector<int> &v, int **dst) {
+    CUDA_TRY(c->upload(dst, v.data(), v.size()));
+    return H2B_OK;
+}
+
+h2b_status build_side(h2b_core *c, const h2b_map_desc &d, const h2b_side_desc &s, const h2b_side_desc &other,
+                      SideHost &h) {
+    h.nnodes = s.nnodes;
+    h.nlevels = s.nlevels;
+    h.ndofs = s.ndofs;
+    h.level.assign(s.level, s.level + s.nnodes);
+    h.shape.assign(s.shape, s.shape + 3 * (s.nlevels + 1));
+    for (int l = 1; l <= s.nlevels; ++l) {
+        h.maxcoef = std::max<int>(h.maxcoef, (int)ncoef_host(s, l));
+        h.maxtsize = std::max<int>(h.maxtsize, (int)tsize_host(s, l));
+        if (l > 1) {
+            int b = 1;
+            for (int k = 0; k < 3; ++k) b *= std::max(s.shape[3 * l + k], s.shape[3 * (l - 1) + k]);
+            h.maxsep = std::max(h.maxsep, b);
+        }
+    }
+    for (int n = 0; n < s.nnodes; ++n) h.maxvals = std::max(h.maxvals, s.value_ptr[n + 1] - s.value_ptr[n]);
+    DSide &D = h.d;
+    D.nnodes = s.nnodes;
+    D.nlevels = s.nlevels;
+    D.ndofs = s.ndofs;
+    int *p;
+    CUDA_TRY(c->upload(&p, s.level, s.nnodes)); D.level = p;
+    CUDA_TRY(c->upload(&p, s.parent, s.nnodes)); D.parent = p;
+    CUDA_TRY(c->upload(&p, s.sector, s.nnodes)); D.sector = p;
+    CUDA_TRY(c->upload(&p, s.child_ptr, s.nnodes + 1)); D.child_ptr = p;
+    CUDA_TRY(c->upload(&p, s.child, s.child_ptr[s.nnodes])); D.child = p;
+    CUDA_TRY(c->upload(&p, s.value_ptr, s.nnodes + 1)); D.value_ptr = p;
+    CUDA_TRY(c->upload(&p, s.value, s.value_ptr[s.nnodes])); D.value = p;
+    CUDA_TRY(c->upload(&p, s.shape, 3 * (s.nlevels + 1))); D.shape = p;
+    CUDA_TRY(c->upload(&p, s.i2o_ptr, s.nnodes + 1)); D.i2o_ptr = p;
+    CUDA_TRY(c->upload(&p, s.i2o_src, s.i2o_ptr[s.nnodes])); D.i2o_src = p;
+    int64_t *q;
+    CUDA_TRY(c->upload(&q, s.i2o_coupling, s.i2o_ptr[s.nnodes])); D.i2o_cpl = q;
+    h.npairs = s.i2o_ptr[s.nnodes];
+
+    // moment / spectrum slots per unit right-hand side
+    std::vector<int64_t> mo(s.nnodes), so(s.nnodes);
+    int64_t mt = 0, stot = 0;
+    const bool toep = d.coupling_kind == H2B_COUPLING_TOEPLITZ;
+    for (int n = 0; n < s.nnodes; ++n) {
+        mo[n] = mt;
+        so[n] = stot;
+        mt += d.ncomp * ncoef_host(s, s.level[n]);
+        if (toep) stot += d.ncomp * tsize_host(s, s.level[n]);
+    }
+    h.mom_total = mt;
+    h.spec_total = stot;
+    CUDA_TRY(c->upload(&q, mo.data(), mo.size())); D.mom_off = q;
+    CUDA_TRY(c->upload(&q, so.data(), so.size())); D.spec_off = q;
+
+    // leaf collections and transfers in the far-field precision
+    const int fw = d.field == H2B_COMPLEX ? 2 : 1;
+    h2b_status st = upload_far_scalars(c, s.coll, s.coll_len, &D.coll);
+    if (st) return st;
+    CUDA_TRY(c->upload(&q, s.coll_offset, s.nnodes)); D.coll_off = q;
+    st = upload_far_scalars(c, s.transfer, s.transfer_len, &D.tr);
+    if (st) return st;
+    CUDA_TRY(c->upload(&q, s.transfer_offset, (size_t)(s.nlevels + 1) * d.nsectors)); D.tr_off = q;
+    (void)fw;
+
+    // node lists
+    std::vector<int> leaves;
+    for (int st2 = 0; st2 < s.agg_nstages; ++st2) {
+        Stage sg;
+        sg.level = s.agg_level[st2];
+        std::vector<int> inner;
+        for (int k = s.agg_ptr[st2]; k < s.agg_ptr[st2 + 1]; ++k) {
+            const int n = s.agg_node[k];
+            if (isleaf(s, n)) leaves.push_back(n);
+            else inner.push_back(n);
+        }
+        sg.n = (int)inner.size();
+        st = upload_list(c, inner, &sg.d_nodes);
+        if (st) return st;
+        h.agg_inner.push_back(sg);
+    }
+    h.n_agg_leaves = (int)leaves.size();
+    st = upload_list(c, leaves, &h.d_agg_leaves);
+    if (st) return st;
+    std::vector<int> store;
+    for (int n = 0; n < s.nnodes; ++n)
+        if (s.agg_store[n]) store.push_back(n);
+    h.n_store = (int)store.size();
+    st = upload_list(c, store, &h.d_store);
+    if (st) return st;
+
+    std::vector<int> recv, initleaves;
+    std::vector<uint8_t> received(s.nnodes, 0);
+    for (int st2 = 0; st2 < s.dis_nstages; ++st2) {
+        Stage sg;
+        sg.level = s.dis_level[st2];
+        std::vector<int> down;
+        for (int k = s.dis_ptr[st2]; k < s.dis_ptr[st2 + 1]; ++k) {
+            const int n = s.dis_node[k];
+            const bool r = s.i2o_ptr[n + 1] > s.i2o_ptr[n];
+            const bool fp = n != s.root && s.dis_isnode[s.parent[n]];
+            if (r) { recv.push_back(n); received[n] = 1; }
+            if (fp) down.push_back(n);
+            if (isleaf(s, n) && (r || fp)) initleaves.push_back(n);
+        }
+        sg.n = (int)down.size();
+        st = upload_list(c, down, &sg.d_nodes);
+        if (st) return st;
+        h.dis_down.push_back(sg);
+    }
+    h.n_recv = (int)recv.size();
+    st = upload_list(c, recv, &h.d_recv);
+    if (st) return st;
+    h.n_init_leaves = (int)initleaves.size();
+    st = upload_list(c, initleaves, &h.d_init_leaves);
+    if (st) return st;
+    CUDA_TRY(c->upload(&h.d_received, received.data(), received.size()));
+    (void)other;
+    return H2B_OK;
+}
+
+h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
+    const int nb = d.near_nrows > 0 ? d.near_ptr[d.near_nrows] : 0;
+    std::vector<int> blk_row(nb), blk_col(nb);
+    std::vector<int64_t> blk_off(nb);
+    int64_t entries = 0;
+    for (int g = 0; g < d.near_nrows; ++g)
+        for (int b = d.near_ptr[g]; b < d.near_ptr[g + 1]; ++b) {
+            blk_row[b] = d.near_row[g];
+            blk_col[b] = d.near_col[b];
+            blk_off[b] = d.near_offset[b];
+            const int64_t nr = d.test.value_ptr[blk_row[b] + 1] - d.test.value_ptr[blk_row[b]];
+            const int64_t nc = d.trial.value_ptr[blk_col[b] + 1] - d.trial.value_ptr[blk_col[b]];
+            entries += nr * nc;
+        }
+    c->near_entries = entries;
+    // groups over every leaf, so that leaves without near blocks still get y = beta * y
+    auto groups = [&](const h2b_side_desc &s, const std::vector<int> &key, std::vector<int> &leaf,
+                      std::vector<int> &ptr, std::vector<int> &blk) {
+        std::vector<int> slot(s.nnodes, -1);
+        for (int n = 0; n < s.nnodes; ++n)
+            if (isleaf(s, n)) { slot[n] = (int)leaf.size(); leaf.push_back(n); }
+        ptr.assign(leaf.size() + 1, 0);
+        for (int b = 0; b < nb; ++b) ptr[slot[key[b]] + 1]++;
+        for (size_t g = 0; g < leaf.size(); ++g) ptr[g + 1] += ptr[g];
+        blk.assign(nb, 0);
+        std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+        for (int b = 0; b < nb; ++b) blk[fill[slot[key[b]]]++] = b;
+    };
+    std::vector<int> rl, rp, rb, cl, cp, cb;
+    groups(d.test, blk_row, rl, rp, rb);
+    groups(d.trial, blk_col, cl, cp, cb);
+    DNear &N = c->dnear;
+    int *p;
+    CUDA_TRY(c->upload(&p, rl.data(), rl.size())); N.row_leaf = p;
+    CUDA_TRY(c->upload(&p, rp.data(), rp.size())); N.row_ptr = p;
+    CUDA_TRY(c->upload(&p, rb.data(), rb.size())); N.row_blk = p;
+    CUDA_TRY(c->upload(&p, cl.data(), cl.size())); N.col_leaf = p;
+    CUDA_TRY(c->upload(&p, cp.data(), cp.size())); N.col_ptr = p;
+    CUDA_TRY(c->upload(&p, cb.data(), cb.size())); N.col_blk = p;
+    CUDA_TRY(c->upload(&p, blk_row.data(), blk_row.size())); N.blk_row = p;
+    CUDA_TRY(c->upload(&p, blk_col.data(), blk_col.size())); N.blk_col = p;
+    int64_t *q;
+    CUDA_TRY(c->upload(&q, blk_off.data(), blk_off.size())); N.blk_off = q;
+    N.nrow_groups = (int)rl.size();
+    N.ncol_groups = (int)cl.size();
+    const size_t vb = d.field == H2B_COMPLEX ? 2 * sizeof(double) : sizeof(double);
+    void *data = nullptr;
+    const size_t bytes = (size_t)std::max<int64_t>(d.near_len, 1) * vb;
+    CUDA_TRY(cudaMalloc(&data, bytes));
+    c->allocs.push_back(data);
+    c->bytes += (int64_t)bytes;
+    if (d.near_len > 0)
+        CUDA_TRY(cudaMemcpy(data, d.near, (size_t)d.near_len * vb,
+                            d.near_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    N.data = data;
+    c->near_maxvals = std::max(c->test.maxvals, c->trial.maxvals);
+    return H2B_OK;
+}
+
+h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
+    h2b_status st = build_side(c, d, d.test, d.trial, c->test);
+    if (st) return st;
+    st = build_side(c, d, d.trial, d.test, c->trial);
+    if (st) return st;
+    DMap &M = c->dmap;
+    M.ncomp = d.ncomp;
+    M.dim = d.dim;
+    M.nsectors = d.nsectors;
+    M.transfer_kind = d.transfer_kind;
+    M.coupling_kind = d.coupling_kind;
+    // coupling data: offsets arrive in doubles; convert to elements of the device type
+    std::vector<int64_t> off(std::max<int64_t>(d.ncouplings, 1), 0);
+    const bool cplx = d.field == H2B_COMPLEX;
+    if (d.coupling_kind == H2B_COUPLING_TOEPLITZ) {
+        for (int64_t k = 0; k < d.ncouplings; ++k) off[k] = d.coupling_offset[k] / 2;
+        const int64_t n = d.coupling_len / 2;
+        if (c->precision == H2B_FP64) st = upload_scalars<cdouble>(c, d.coupling, n, &M.cpl);
+        else st = upload_scalars<cfloat>(c, d.coupling, n, &M.cpl);
+    } else {
+        const int fw = cplx ? 2 : 1;
+        for (int64_t k = 0; k < d.ncouplings; ++k) off[k] = d.coupling_offset[k] / fw;
+        st = upload_far_scalars(c, d.coupling, d.coupling_len / fw, &M.cpl);
+    }
+    if (st) return st;
+    int64_t *q;
+    CUDA_TRY(c->upload(&q, off.data(), off.size()));
+    M.cpl_off = q;
+    return build_near(c, d);
+}
+
+}  // namespace
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+extern "C" {
+
+int32_t h2b_version(void) { return (1 << 16) | 0; }
+
+const char *h2b_last_error(void) { return g_err.c_str(); }
+
+h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **out) {
+    if (!desc || !out) return fail(H2B_ERR_INVALID, "null argument");
+    *out = nullptr;
+    try {
+        h2b_status st = validate(*desc);
+        if (st) return st;
+        int ndev = 0;
+        CUDA_TRY(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev) return fail(H2B_ERR_INVALID, "device %d not present", device);
+        DeviceGuard guard(device);
+        h2b_core *c = new h2b_core();
+        c->device = device;
+        c->field = desc->field;
+        c->precision = desc->precision;
+        c->conj_leaf = desc->conj_leaf_adjoint != 0;
+        for (int m = 0; m < 3; ++m) c->alpha[m] = {desc->alpha[m][0], desc->alpha[m][1]};
+        st = build_core(c, *desc);
+        if (st) {
+            c->release();
+            delete c;
+            return st;
+        }
+        *out = c;
+        return H2B_OK;
+    } catch (const std::bad_alloc &) {
+        return fail(H2B_ERR_NOMEM, "host allocation failed");
+    } catch (...) {
+        return fail(H2B_ERR_INVALID, "unexpected exception in h2b_core_create");
+    }
+}
+
+h2b_status h2b_core_destroy(h2b_core *core) {
+    if (!core) return H2B_OK;
+    DeviceGuard guard(core->device);
+    core->release();
+    delete core;
+    return H2B_OK;
+}
+
+h2b_status h2b_core_get_info(const h2b_core *core, h2b_core_info *out) {
+    if (!core || !out) return fail(H2B_ERR_INVALID, "null argument");
+    out->device_bytes = core->bytes;
+    out->near_entries = core->near_entries;
+    out->npairs[0] = core->test.npairs;
+    out->npairs[1] = core->trial.npairs;
+    out->moment_elems = std::max(core->test.mom_total, core->trial.mom_total);
+    out->spectrum_elems = std::max(core->test.spec_total, core->trial.spec_total);
+    out->nrows = core->test.ndofs;
+    out->ncols = core->trial.ndofs;
+    return H2B_OK;
+}
+
+h2b_status h2b_workspace_destroy(h2b_workspace *ws) {
+    if (!ws) return H2B_OK;
+    DeviceGuard guard(ws->core->device);
+    if (ws->ev_done) cudaEventSynchronize(ws->ev_done);
+    for (void *p : ws->allocs) cudaFree(p);
+    if (ws->aux) cudaStreamDestroy(ws->aux);
+    if (ws->ev_fork) cudaEventDestroy(ws->ev_fork);
+    if (ws->ev_join) cudaEventDestroy(ws->ev_join);
+    if (ws->ev_done) cudaEventDestroy(ws->ev_done);
+    delete ws;
+    return H2B_OK;
+}
+
+h2b_status h2b_workspace_create(h2b_core *core, int32_t max_nrhs, h2b_workspace **out) {
+    if (!core || !out) return fail(H2B_ERR_INVALID, "null argument");
+    if (max_nrhs < 1) return fail(H2B_ERR_INVALID, "max_nrhs must be >= 1");
+    *out = nullptr;
+    DeviceGuard guard(core->device);
+    h2b_workspace *ws = new (std::nothrow) h2b_workspace();
+    if (!ws) return fail(H2B_ERR_NOMEM, "host allocation failed");
+    ws->core = core;
+    ws->max_nrhs = max_nrhs;
+    const bool cplx = core->field == H2B_COMPLEX;
+    const size_t tsz = (cplx ? 2 : 1) * (core->precision == H2B_FP64 ? 8 : 4);
+    const size_t ssz = 2 * (core->precision == H2B_FP64 ? 8 : 4);
+    const size_t vsz = cplx ? 16 : 8;
+    const int64_t mom = std::max(core->test.mom_total, core->trial.mom_total) * max_nrhs;
+    const int64_t spec = std::max(core->test.spec_total, core->trial.spec_total) * max_nrhs;
+    const int64_t ndof = std::max(core->test.ndofs, core->trial.ndofs) * (int64_t)max_nrhs;
+    auto al = [&](void **p, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+        if (e == cudaSuccess) ws->allocs.push_back(*p);
+        return e;
+    };
+    cudaError_t e = al(&ws->am, mom * tsz);
+    if (e == cudaSuccess) e = al(&ws->dm, mom * tsz);
+    if (e == cudaSuccess) e = al(&ws->as, spec * ssz);
+    if (e == cudaSuccess) e = al(&ws->ds, spec * ssz);
+    if (e == cudaSuccess) e = al(&ws->xbuf, ndof * vsz);
+    if (e == cudaSuccess) e = al(&ws->ybuf, ndof * vsz);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ws->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        h2b_workspace_destroy(ws);
+        return fail(e == cudaErrorMemoryAllocation ? H2B_ERR_NOMEM : H2B_ERR_CUDA,
+                    "workspace allocation failed: %s", cudaGetErrorString(e));
+    }
+    *out = ws;
+    return H2B_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+enum Kind { KIND_MATVEC, KIND_FAR, KIND_NEAR };
+
+struct BusyGuard {
+    std::atomic<int> &flag;
+    bool ok;
+    explicit BusyGuard(std::atomic<int> &f) : flag(f) {
+        int expect = 0;
+        ok = flag.compare_exchange_strong(expect, 1);
+    }
+    ~BusyGuard() {
+        if (ok) flag.store(0);
+    }
+};
+
+h2b_status far_passes(h2b_workspace *ws, int mode, int nrhs, const void *x, int64_t ldx, void *y,
+                      int64_t ldy, cdouble alpha_eff, cdouble beta, cudaStream_t st,
+                      cudaEvent_t wait_before_scatter) {
+    h2b_core *c = ws->core;
+    const SideHost &A = mode == H2B_FORWARD ? c->trial : c->test;
+    const SideHost &D = mode == H2B_FORWARD ? c->test : c->trial;
+    const bool cplx = c->field == H2B_COMPLEX;
+    const int pr = c->precision;
+    FarArgs fa{mode, nrhs, ws->am, ws->dm, ws->as, ws->ds};
+    const bool conjc = mode == H2B_ADJOINT && c->conj_leaf;
+    const bool toep = c->dmap.coupling_kind == H2B_COUPLING_TOEPLITZ;
+    const int maxcoef = std::max(A.maxcoef, D.maxcoef);
+    const int maxt = std::max(A.maxtsize, D.maxtsize);
+    CUDA_TRY(launch_leaf_aggregate(cplx, pr, c->dmap, A.d, A.d_agg_leaves, A.n_agg_leaves, A.maxcoef,
+                                   conjc, fa, x, ldx, st));
+    for (const Stage &sg : A.agg_inner)
+        CUDA_TRY(launch_transfer_up(cplx, pr, c->dmap, A.d, sg.d_nodes, sg.n, mode == H2B_ADJOINT, fa,
+                                    A.maxcoef, A.maxsep, st));
+    if (toep)
+        CUDA_TRY(launch_toeplitz_in(cplx, pr, c->dmap, A.d, A.d_store, A.n_store, mode == H2B_TRANSPOSE,
+                                    fa, A.maxtsize, st));
+    CUDA_TRY(launch_i2o(cplx, pr, c->dmap, D.d, A.d, D.d_recv, D.n_recv, fa, maxcoef, maxt, st));
+    if (toep)
+        CUDA_TRY(launch_toeplitz_out(cplx, pr, c->dmap, D.d, D.d_recv, D.n_recv, mode != H2B_TRANSPOSE,
+                                     fa, D.maxtsize, st));
+    for (const Stage &sg : D.dis_down)
+        CUDA_TRY(launch_transfer_down(cplx, pr, c->dmap, D.d, sg.d_nodes, sg.n, D.d_received, fa,
+                                      D.maxcoef, D.maxsep, st));
+    if (wait_before_scatter) CUDA_TRY(cudaStreamWaitEvent(st, wait_before_scatter, 0));
+    CUDA_TRY(launch_leaf_disaggregate(cplx, pr, c->dmap, D.d, D.d_init_leaves, D.n_init_leaves, conjc,
+                                      fa, alpha_eff, beta, y, ldy, st));
+    return H2B_OK;
+}
+
+cdouble cmul(cdouble a, cdouble b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+
+h2b_status run(h2b_workspace *ws, Kind kind, int32_t mode, int32_t nrhs, const void *x, int64_t ldx,
+               void *y, int64_t ldy, const double *alpha, const double *beta, void *stream,
+               bool take_busy = true) {
+    if (!ws) return fail(H2B_ERR_INVALID, "null workspace");
+    if (mode < 0 || mode > 2) return fail(H2B_ERR_INVALID, "mode must be 0, 1 or 2");
+    if (nrhs < 1 || nrhs > ws->max_nrhs)
+        return fail(H2B_ERR_INVALID, "nrhs = %d outside 1..%d (workspace max_nrhs)", nrhs, ws->max_nrhs);
+    if ((alpha == nullptr) != (beta == nullptr))
+        return fail(H2B_ERR_INVALID, "alpha and beta must both be given or both be NULL");
+    h2b_core *c = ws->core;
+    const int64_t nout = mode == H2B_FORWARD ? c->test.ndofs : c->trial.ndofs;
+    const int64_t nin = mode == H2B_FORWARD ? c->trial.ndofs : c->test.ndofs;
+    if (!x || !y) return fail(H2B_ERR_INVALID, "null x or y");
+    if (ldx < nin || ldy < nout) return fail(H2B_ERR_INVALID, "leading dimension smaller than the vector length");
+    if (c->field == H2B_REAL && alpha && (alpha[1] != 0.0 || beta[1] != 0.0))
+        return fail(H2B_ERR_INVALID, "complex alpha/beta on a real map");
+    BusyGuard busy(ws->busy);
+    if (take_busy && !busy.ok) return fail(H2B_BUSY, "workspace is in use by another call");
+    DeviceGuard guard(c->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // serialise with the previous call on this workspace, whatever stream it used
+    CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_done, 0));
+    const cdouble a = alpha ? cdouble{alpha[0], alpha[1]} : cdouble{1.0, 0.0};
+    const cdouble b = beta ? cdouble{beta[0], beta[1]} : cdouble{0.0, 0.0};
+    const cdouble aA = c->alpha[mode];
+    const bool cplx = c->field == H2B_COMPLEX;
+    const SideHost &rows = c->test;
+    const SideHost &cols = c->trial;
+    h2b_status s = H2B_OK;
+    if (kind == KIND_NEAR) {
+        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b,
+                             c->near_maxvals, st));
+    } else if (kind == KIND_FAR) {
+        if (!alpha) {
+            CUDA_TRY(launch_zero_columns(cplx, nrhs, nout, y, ldy, st));
+            s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, aA, cdouble{0.0, 0.0}, st, nullptr);
+        } else {
+            s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(aA, a), b, st, nullptr);
+        }
+    } else {
+        // near on the auxiliary stream, far on the caller's; the leaf scatter waits for the near
+        CUDA_TRY(cudaEventRecord(ws->ev_fork, st));
+        CUDA_TRY(cudaStreamWaitEvent(ws->aux, ws->ev_fork, 0));
+        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b,
+                             c->near_maxvals, ws->aux));
+        CUDA_TRY(cudaEventRecord(ws->ev_join, ws->aux));
+        s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(aA, a), cdouble{1.0, 0.0}, st, ws->ev_join);
+    }
+    if (s) return s;
+    CUDA_TRY(cudaEventRecord(ws->ev_done, st));
+    return H2B_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+h2b_status h2b_matvec(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x, int64_t ldx,
+                      void *y, int64_t ldy, const double *alpha, const double *beta, void *stream) {
+    return run(ws, KIND_MATVEC, mode, nrhs, x, ldx, y, ldy, alpha, beta, stream);
+}
+
+h2b_status h2b_farmul(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x, int64_t ldx,
+                      void *y, int64_t ldy, const double *alpha, const double *beta, void *stream) {
+    return run(ws, KIND_FAR, mode, nrhs, x, ldx, y, ldy, alpha, beta, stream);
+}
+
+h2b_status h2b_nearmul(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x, int64_t ldx,
+                       void *y, int64_t ldy, const double *alpha, const double *beta, void *stream) {
+    return run(ws, KIND_NEAR, mode, nrhs, x, ldx, y, ldy, alpha, beta, stream);
+}
+
+h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
+                           int64_t ldx, void *y, int64_t ldy, const double *alpha,
+                           const double *beta, void *stream) {
+    if (!ws || !x || !y) return fail(H2B_ERR_INVALID, "null argument");
+    if (mode < 0 || mode > 2) return fail(H2B_ERR_INVALID, "mode must be 0, 1 or 2");
+    if (nrhs < 1 || nrhs > ws->max_nrhs)
+        return fail(H2B_ERR_INVALID, "nrhs = %d outside 1..%d (workspace max_nrhs)", nrhs, ws->max_nrhs);
+    h2b_core *c = ws->core;
+    const int64_t nout = mode == H2B_FORWARD ? c->test.ndofs : c->trial.ndofs;
+    const int64_t nin = mode == H2B_FORWARD ? c->trial.ndofs : c->test.ndofs;
+    if (ldx < nin || ldy < nout) return fail(H2B_ERR_INVALID, "leading dimension smaller than the vector length");
+    const size_t vsz = c->field == H2B_COMPLEX ? 16 : 8;
+    BusyGuard busy(ws->busy);
+    if (!busy.ok) return fail(H2B_BUSY, "workspace is in use by another call");
+    DeviceGuard guard(c->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_done, 0));
+    CUDA_TRY(cudaMemcpy2DAsync(ws->xbuf, nin * vsz, x, ldx * vsz, nin * vsz, nrhs, cudaMemcpyHostToDevice, st));
+    const bool need_y = beta && (beta[0] != 0.0 || beta[1] != 0.0);
+    if (need_y)
+        CUDA_TRY(cudaMemcpy2DAsync(ws->ybuf, nout * vsz, y, ldy * vsz, nout * vsz, nrhs, cudaMemcpyHostToDevice, st));
+    h2b_status s = run(ws, KIND_MATVEC, mode, nrhs, ws->xbuf, nin, ws->ybuf, nout, alpha, beta, stream,
+                       /*take_busy=*/false);
+    if (s) return s;
+    CUDA_TRY(cudaMemcpy2DAsync(y, ldy * vsz, ws->ybuf, nout * vsz, nout * vsz, nrhs, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return H2B_OK;
+}
+
+}  // extern "C"

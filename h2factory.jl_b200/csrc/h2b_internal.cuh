@@ -1,0 +1,145 @@
+// Internal definitions shared by the host orchestration (h2b_api.cu) and the kernels
+// (h2b_kernels.cu): scalar types, the device-resident core layout, and kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/h2b200.h"
+
+namespace h2b {
+
+// ---------------------------------------------------------------------------------------------
+// Scalars. V is the field type of x, y and the near blocks (double or cdouble); T is the far-field
+// arithmetic type (double, float, cdouble or cfloat); Toeplitz spectra are complex of T's real type.
+// ---------------------------------------------------------------------------------------------
+template <class R>
+struct Cx {
+    R x, y;
+};
+using cdouble = Cx<double>;
+using cfloat = Cx<float>;
+
+template <class T> struct ScalarTraits;
+template <> struct ScalarTraits<double> { using Real = double; using Complex = cdouble; static constexpr bool is_complex = false; };
+template <> struct ScalarTraits<float> { using Real = float; using Complex = cfloat; static constexpr bool is_complex = false; };
+template <> struct ScalarTraits<cdouble> { using Real = double; using Complex = cdouble; static constexpr bool is_complex = true; };
+template <> struct ScalarTraits<cfloat> { using Real = float; using Complex = cfloat; static constexpr bool is_complex = true; };
+
+template <class R> __host__ __device__ __forceinline__ Cx<R> operator+(Cx<R> a, Cx<R> b) { return {a.x + b.x, a.y + b.y}; }
+template <class R> __host__ __device__ __forceinline__ Cx<R> operator-(Cx<R> a, Cx<R> b) { return {a.x - b.x, a.y - b.y}; }
+template <class R> __host__ __device__ __forceinline__ Cx<R> operator*(Cx<R> a, Cx<R> b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <class R> __host__ __device__ __forceinline__ Cx<R> operator*(R a, Cx<R> b) { return {a * b.x, a * b.y}; }
+template <class R> __host__ __device__ __forceinline__ Cx<R> &operator+=(Cx<R> &a, Cx<R> b) { a.x += b.x; a.y += b.y; return a; }
+
+__host__ __device__ __forceinline__ double conjg(double a) { return a; }
+__host__ __device__ __forceinline__ float conjg(float a) { return a; }
+template <class R> __host__ __device__ __forceinline__ Cx<R> conjg(Cx<R> a) { return {a.x, -a.y}; }
+
+template <class T> __host__ __device__ __forceinline__ T sc_zero() { return T{}; }
+template <class T> __host__ __device__ __forceinline__ bool is_zero(T a);
+template <> __host__ __device__ __forceinline__ bool is_zero(double a) { return a == 0.0; }
+template <> __host__ __device__ __forceinline__ bool is_zero(cdouble a) { return a.x == 0.0 && a.y == 0.0; }
+
+// optional conjugation
+template <class T> __host__ __device__ __forceinline__ T cj(T a, bool c) { return c ? conjg(a) : a; }
+
+// conversions between the field type V and the far type T (same complexness)
+__host__ __device__ __forceinline__ double to_t(double v, double) { return v; }
+__host__ __device__ __forceinline__ float to_t(double v, float) { return (float)v; }
+__host__ __device__ __forceinline__ cdouble to_t(cdouble v, cdouble) { return v; }
+__host__ __device__ __forceinline__ cfloat to_t(cdouble v, cfloat) { return {(float)v.x, (float)v.y}; }
+__host__ __device__ __forceinline__ double to_v(double t) { return t; }
+__host__ __device__ __forceinline__ double to_v(float t) { return (double)t; }
+__host__ __device__ __forceinline__ cdouble to_v(cdouble t) { return t; }
+__host__ __device__ __forceinline__ cdouble to_v(cfloat t) { return {(double)t.x, (double)t.y}; }
+// moment <-> spectrum
+template <class R> __host__ __device__ __forceinline__ Cx<R> to_cx(R a) { return {a, (R)0}; }
+template <class R> __host__ __device__ __forceinline__ Cx<R> to_cx(Cx<R> a) { return a; }
+template <class R> __host__ __device__ __forceinline__ void from_cx(Cx<R> s, R &out) { out = s.x; }
+template <class R> __host__ __device__ __forceinline__ void from_cx(Cx<R> s, Cx<R> &out) { out = s; }
+
+// ---------------------------------------------------------------------------------------------
+// Device-resident side of a core (all pointers device memory).
+// ---------------------------------------------------------------------------------------------
+struct DSide {
+    int nnodes, nlevels, ndofs;
+    const int *level, *parent, *sector, *child_ptr, *child, *value_ptr, *value;
+    const int *shape;        // [(nlevels+1)*3]
+    const int64_t *mom_off;  // [nnodes] moment offset per unit right-hand side (elements of T)
+    const int64_t *spec_off; // [nnodes] spectrum offset per unit right-hand side (complex elements)
+    const int64_t *coll_off; // [nnodes] leaf collection offsets (elements of T)
+    const void *coll;        // T
+    const int64_t *tr_off;   // [(nlevels+1)*nsectors] transfer offsets (elements of T)
+    const void *tr;          // T
+    const int *i2o_ptr, *i2o_src;
+    const int64_t *i2o_cpl;  // coupling index of each pair
+};
+
+struct DMap {
+    int ncomp, dim, nsectors;
+    int transfer_kind, coupling_kind;
+    const int64_t *cpl_off;  // [ncouplings] offsets in elements of T (dense/diag) or spectrum (Toeplitz)
+    const void *cpl;
+};
+
+// Near blocks in block-CSR by test leaf (forward) and block-CSC by trial leaf (transposed).
+struct DNear {
+    const int *row_leaf;   // [nrow_groups] test leaf of each group (covers every test leaf)
+    const int *row_ptr;    // [nrow_groups+1]
+    const int *row_blk;    // block ids
+    const int *col_leaf;   // [ncol_groups] trial leaf of each group (covers every trial leaf)
+    const int *col_ptr;
+    const int *col_blk;
+    const int *blk_row;    // [nblocks] test leaf of block
+    const int *blk_col;    // [nblocks] trial leaf of block
+    const int64_t *blk_off;
+    const void *data;      // V
+    int nrow_groups, ncol_groups;
+};
+
+// Per-call arguments of the far passes.
+struct FarArgs {
+    int mode;     // H2B_FORWARD / H2B_TRANSPOSE / H2B_ADJOINT
+    int nrhs;
+    void *am;     // aggregation moments (T)
+    void *dm;     // disaggregation moments (T)
+    void *as;     // aggregation spectra (complex of T's real)
+    void *ds;     // disaggregation spectra
+};
+
+// ---------------------------------------------------------------------------------------------
+// Launchers (h2b_kernels.cu). Each enqueues on `st` and returns the launch error.
+// `precision`: 0 = T is FP64, 1 = FP32; `cplx`: field is complex.
+// ---------------------------------------------------------------------------------------------
+cudaError_t launch_leaf_aggregate(bool cplx, int precision, const DMap &m, const DSide &s,
+                                  const int *leaves, int nleaves, int maxcoef, bool conjc,
+                                  const FarArgs &fa, const void *x, int64_t ldx, cudaStream_t st);
+cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DSide &s,
+                               const int *nodes, int nnodes, bool conjt, const FarArgs &fa,
+                               int maxcoef, int maxsep, cudaStream_t st);
+cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DSide &s,
+                               const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
+                               int maxtsize, cudaStream_t st);
+cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &recv,
+                       const DSide &src, const int *nodes, int nnodes, const FarArgs &fa,
+                       int maxcoef, int maxtsize, cudaStream_t st);
+cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const DSide &s,
+                                const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
+                                int maxtsize, cudaStream_t st);
+cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const DSide &s,
+                                 const int *nodes, int nnodes, const uint8_t *received,
+                                 const FarArgs &fa, int maxcoef, int maxsep, cudaStream_t st);
+cudaError_t launch_leaf_disaggregate(bool cplx, int precision, const DMap &m, const DSide &s,
+                                     const int *leaves, int nleaves, bool conjc, const FarArgs &fa,
+                                     cdouble alpha, cdouble beta, void *y, int64_t ldy,
+                                     cudaStream_t st);
+cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &rows,
+                        const DSide &cols, int nrhs, const void *x, int64_t ldx, void *y,
+                        int64_t ldy, cdouble alpha, cdouble beta, int maxvals, cudaStream_t st);
+cudaError_t launch_zero_columns(bool cplx, int nrhs, int64_t n, void *y, int64_t ldy,
+                                cudaStream_t st);
+
+}  // namespace h2b

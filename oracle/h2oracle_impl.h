@@ -406,22 +406,40 @@ static int SFX(farmul)(const h2b_map_desc *d, int mode, int nrhs, const SC *x, i
 /* ---------------------------------------------------------------------------------------------
  * Near product: y = α op(N) x + β y with the SparseMatrixCSC rule: β scales (or, when zero,
  * clears) all of y first, then α N x is added (nearmul.jl:8-14, accessors.jl:149-159).
+ * Blocks are grouped by the leaf that owns their output rows, so output leaves run in parallel.
  * ------------------------------------------------------------------------------------------- */
 static int SFX(nearmul)(const h2b_map_desc *d, int mode, int nrhs, const SC *x, int64_t ldx, SC *y,
                         int64_t ldy, SC alpha, SC beta) {
     const h2b_side_desc *rs = &d->test, *cs = &d->trial;
-    const int64_t ny = (mode == H2B_FORWARD) ? rs->ndofs : cs->ndofs;
+    const h2b_side_desc *os = (mode == H2B_FORWARD) ? rs : cs;
+    const int64_t ny = os->ndofs;
     for (int r = 0; r < nrhs; ++r)
         for (int64_t i = 0; i < ny; ++i) {
             SC *v = &y[(int64_t)r * ldy + i];
             *v = (beta == 0) ? 0 : beta * *v;
         }
+    const int nb = d->near_nrows > 0 ? d->near_ptr[d->near_nrows] : 0;
+    int *brow = (int *)malloc(sizeof(int) * (size_t)(nb + 1));
+    int *ptr = (int *)calloc((size_t)os->nnodes + 1, sizeof(int));
+    int *order = (int *)malloc(sizeof(int) * (size_t)(nb + 1));
+    if (!brow || !ptr || !order) { free(brow); free(ptr); free(order); oracle_set_error("out of host memory"); return H2B_ERR_NOMEM; }
+    for (int g = 0; g < d->near_nrows; ++g)
+        for (int b = d->near_ptr[g]; b < d->near_ptr[g + 1]; ++b) brow[b] = d->near_row[g];
+    for (int b = 0; b < nb; ++b) ptr[(mode == H2B_FORWARD ? brow[b] : d->near_col[b]) + 1]++;
+    for (int n = 0; n < os->nnodes; ++n) ptr[n + 1] += ptr[n];
+    {
+        int *fill = (int *)malloc(sizeof(int) * (size_t)(os->nnodes + 1));
+        memcpy(fill, ptr, sizeof(int) * (size_t)(os->nnodes + 1));
+        for (int b = 0; b < nb; ++b) order[fill[mode == H2B_FORWARD ? brow[b] : d->near_col[b]]++] = b;
+        free(fill);
+    }
     const SC *N = (const SC *)d->near;
-    for (int g = 0; g < d->near_nrows; ++g) {
-        const int row = d->near_row[g];
-        const int r0 = rs->value_ptr[row], nr = rs->value_ptr[row + 1] - r0;
-        for (int b = d->near_ptr[g]; b < d->near_ptr[g + 1]; ++b) {
-            const int col = d->near_col[b];
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int leaf = 0; leaf < os->nnodes; ++leaf) {
+        for (int k = ptr[leaf]; k < ptr[leaf + 1]; ++k) {
+            const int b = order[k];
+            const int row = brow[b], col = d->near_col[b];
+            const int r0 = rs->value_ptr[row], nr = rs->value_ptr[row + 1] - r0;
             const int c0 = cs->value_ptr[col], nc = cs->value_ptr[col + 1] - c0;
             const SC *B = N + d->near_offset[b];
             for (int q = 0; q < nrhs; ++q) {
@@ -446,5 +464,8 @@ static int SFX(nearmul)(const h2b_map_desc *d, int mode, int nrhs, const SC *x, 
             }
         }
     }
+    free(brow);
+    free(ptr);
+    free(order);
     return H2B_OK;
 }
