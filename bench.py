@@ -272,7 +272,7 @@ def gpu_arm(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     device = f"cuda:{local_rank}"
-    h2, core = build_core(device=device, precision="fp64")
+    h2, core = build_core(n=args.n, depth=args.depth, device=device, precision="fp64")
     nrhs = args.nrhs
     ws = h2.H2Workspace(core, max_nrhs=nrhs, device=local_rank)
     n = core.trial.npoints
@@ -355,7 +355,8 @@ def gpu_arm(args, rank, world, local_rank):
     near_bytes = info.near_entries * 8 + 2 * n * 8 * nrhs
     near_ms = ntotal / len(nper)
     achieved = near_bytes / (near_ms * 1e-3) / 1e9
-    traffic = traffic_table().get(("near_forward_kernel", WORKLOAD))
+    workload = WORKLOAD if (args.n, args.depth) == (262144, 5) else f"toeplitz-laplace-N{args.n}-depth{args.depth}-p4"
+    traffic = traffic_table().get(("near_forward_kernel", workload))
     launches = sum(launches_per_step(core, i % 2) for i in range(args.steps))
     rhs_total = args.steps * nrhs * world
     line = {
@@ -363,7 +364,7 @@ def gpu_arm(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tmax / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded uniform points in the unit cube)",
-        "config": {"workload": WORKLOAD, "form": "plain (FP64 far and near)", "rhs_per_step": nrhs,
+        "config": {"workload": workload, "form": "plain (FP64 far and near)", "rhs_per_step": nrhs,
                    "modes": "forward/transpose alternating", "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (3.2 GB near blocks); no flush",
                    "near_entries": int(info.near_entries), "i2o_pairs": int(info.npairs[0])},
@@ -400,6 +401,8 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-check", action="store_true")
+    ap.add_argument("--n", type=int, default=262144, help="points (smaller cases are for profiling)")
+    ap.add_argument("--depth", type=int, default=5)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
