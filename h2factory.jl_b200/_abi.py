@@ -71,8 +71,10 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 EXPORTS = [
     "h2b_version", "h2b_last_error", "h2b_core_create", "h2b_core_destroy", "h2b_core_get_info",
     "h2b_workspace_create", "h2b_workspace_destroy", "h2b_matvec", "h2b_matvec_host",
-    "h2b_farmul", "h2b_nearmul",
+    "h2b_farmul", "h2b_nearmul", "h2b_farmul_noalloc",
 ]
+
+H2B_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 class H2BError(RuntimeError):
@@ -111,6 +113,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     mv = [vp, C.c_int32, C.c_int32, vp, C.c_int64, vp, C.c_int64, _f64p, _f64p, vp]
     for name in ("h2b_matvec", "h2b_matvec_host", "h2b_farmul", "h2b_nearmul"):
         getattr(lib, name).argtypes = mv
+    # far part in the library's built-in scratch: takes the core instead of a workspace
+    lib.h2b_farmul_noalloc.argtypes = mv
     for name in EXPORTS:
         if name not in ("h2b_version", "h2b_last_error"):
             getattr(lib, name).restype = C.c_int

@@ -880,3 +880,125 @@ h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const 
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Far part in the library's own scratch: h2b_farmul_noalloc.
+//
+// For callers that cannot allocate device memory when they multiply (their GPU memory belongs to
+// another allocator, or allocation is forbidden after start-up): the moment and spectrum arenas
+// that a workspace would allocate are carved out of one array compiled into this file instead.
+// =============================================================================================
+#include <mutex>
+
+namespace {
+
+// The scratch array (H2B_NOALLOC_SCRATCH_BYTES on every device that loads the library, until the
+// process exits). Device code may name it directly; host code must not pass `g_noalloc_scratch`
+// itself to a kernel -- on the host that name is only a stand-in, not a device address -- and
+// asks the runtime for the address on each device instead (noalloc_scratch below).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[H2B_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on `device`, which must be the current device. Looked up
+// on the first call per device and cached; that first call should precede any stream capture.
+h2b_status noalloc_scratch(int device, void **out) {
+    if (device < 0 || device >= kNoallocMaxDevices)
+        return fail(H2B_ERR_UNSUPPORTED, "no-alloc scratch: device %d beyond the supported %d", device,
+                    kNoallocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            return fail(H2B_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
+                        cudaGetErrorString(e));
+        g_noalloc_ptr[device] = p;
+    }
+    *out = g_noalloc_ptr[device];
+    return H2B_OK;
+}
+
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// The far passes of far_passes() with the arenas given in `fa` (no workspace, caller's stream).
+h2b_status far_passes_scratch(h2b_core *c, const FarArgs &fa, const void *x, int64_t ldx, void *y,
+                              int64_t ldy, cdouble alpha_eff, cdouble beta, cudaStream_t st) {
+    const int mode = fa.mode;
+    const SideHost &A = mode == H2B_FORWARD ? c->trial : c->test;
+    const SideHost &D = mode == H2B_FORWARD ? c->test : c->trial;
+    const bool cplx = c->field == H2B_COMPLEX;
+    const int pr = c->precision;
+    const bool conjc = mode == H2B_ADJOINT && c->conj_leaf;
+    const bool toep = c->dmap.coupling_kind == H2B_COUPLING_TOEPLITZ;
+    const int maxcoef = std::max(A.maxcoef, D.maxcoef);
+    const int maxt = std::max(A.maxtsize, D.maxtsize);
+    CUDA_TRY(launch_leaf_aggregate(cplx, pr, c->dmap, A.d, A.d_agg_leaves, A.n_agg_leaves, A.maxcoef,
+                                   conjc, fa, x, ldx, st));
+    for (const Stage &sg : A.agg_inner)
+        CUDA_TRY(launch_transfer_up(cplx, pr, c->dmap, A.d, sg.d_nodes, sg.n, mode == H2B_ADJOINT, fa,
+                                    A.maxcoef, A.maxsep, st));
+    if (toep)
+        CUDA_TRY(launch_toeplitz_in(cplx, pr, c->dmap, A.d, A.d_store, A.n_store, mode == H2B_TRANSPOSE,
+                                    fa, A.maxtsize, st));
+    CUDA_TRY(launch_i2o(cplx, pr, c->dmap, D.d, A.d, D.d_recv, D.n_recv, fa, maxcoef, maxt, st));
+    if (toep)
+        CUDA_TRY(launch_toeplitz_out(cplx, pr, c->dmap, D.d, D.d_recv, D.n_recv, mode != H2B_TRANSPOSE,
+                                     fa, D.maxtsize, st));
+    for (const Stage &sg : D.dis_down)
+        CUDA_TRY(launch_transfer_down(cplx, pr, c->dmap, D.d, sg.d_nodes, sg.n, D.d_received, fa,
+                                      D.maxcoef, D.maxsep, st));
+    CUDA_TRY(launch_leaf_disaggregate(cplx, pr, c->dmap, D.d, D.d_init_leaves, D.n_init_leaves, conjc,
+                                      fa, alpha_eff, beta, y, ldy, st));
+    return H2B_OK;
+}
+
+}  // namespace
+
+extern "C" h2b_status h2b_farmul_noalloc(const h2b_core *core_in, int32_t mode, int32_t nrhs,
+                                         const void *x, int64_t ldx, void *y, int64_t ldy,
+                                         const double *alpha, const double *beta, void *stream) {
+    h2b_core *c = const_cast<h2b_core *>(core_in);
+    if (!c) return fail(H2B_ERR_INVALID, "null core");
+    if (mode < 0 || mode > 2) return fail(H2B_ERR_INVALID, "mode must be 0, 1 or 2");
+    if (nrhs < 1) return fail(H2B_ERR_INVALID, "nrhs must be >= 1");
+    if ((alpha == nullptr) != (beta == nullptr))
+        return fail(H2B_ERR_INVALID, "alpha and beta must both be given or both be NULL");
+    if (!x || !y) return fail(H2B_ERR_INVALID, "null x or y");
+    const int64_t nout = mode == H2B_FORWARD ? c->test.ndofs : c->trial.ndofs;
+    const int64_t nin = mode == H2B_FORWARD ? c->trial.ndofs : c->test.ndofs;
+    if (ldx < nin || ldy < nout) return fail(H2B_ERR_INVALID, "leading dimension smaller than the vector length");
+    if (c->field == H2B_REAL && alpha && (alpha[1] != 0.0 || beta[1] != 0.0))
+        return fail(H2B_ERR_INVALID, "complex alpha/beta on a real map");
+    // scratch layout: aggregation moments, disaggregation moments, then (Toeplitz) both spectra
+    const bool cplx = c->field == H2B_COMPLEX;
+    const size_t tsz = (cplx ? 2 : 1) * (c->precision == H2B_FP64 ? 8 : 4);
+    const size_t ssz = 2 * (c->precision == H2B_FP64 ? 8 : 4);
+    const size_t mom = align256((size_t)std::max(c->test.mom_total, c->trial.mom_total) * nrhs * tsz);
+    const size_t spec = align256((size_t)std::max(c->test.spec_total, c->trial.spec_total) * nrhs * ssz);
+    const size_t need = 2 * mom + 2 * spec;
+    if (need > (size_t)H2B_NOALLOC_SCRATCH_BYTES)
+        return fail(H2B_ERR_UNSUPPORTED,
+                    "h2b_farmul_noalloc: this map needs %zu bytes of scratch for %d right-hand side(s); "
+                    "the built-in scratch holds %u bytes (use a workspace and h2b_farmul instead)",
+                    need, nrhs, (unsigned)H2B_NOALLOC_SCRATCH_BYTES);
+    DeviceGuard guard(c->device);
+    void *base = nullptr;
+    h2b_status s = noalloc_scratch(c->device, &base);
+    if (s) return s;
+    unsigned char *b = static_cast<unsigned char *>(base);
+    // Nothing in the scratch needs clearing: every pass overwrites a moment or spectrum slot
+    // before any pass reads it (leaf products and first-child / first-pair writes overwrite),
+    // so whatever the previous call left there is never read.
+    FarArgs fa{mode, nrhs, b, b + mom, b + 2 * mom, b + 2 * mom + spec};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const cdouble aA = c->alpha[mode];
+    if (!alpha) {
+        CUDA_TRY(launch_zero_columns(cplx, nrhs, nout, y, ldy, st));
+        return far_passes_scratch(c, fa, x, ldx, y, ldy, aA, cdouble{0.0, 0.0}, st);
+    }
+    return far_passes_scratch(c, fa, x, ldx, y, ldy, cmul(aA, cdouble{alpha[0], alpha[1]}),
+                              cdouble{beta[0], beta[1]}, st);
+}

@@ -225,6 +225,33 @@ h2b_status h2b_nearmul(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void
                        int64_t ldx, void *y, int64_t ldy, const double *alpha,
                        const double *beta, void *stream);
 
+/* Size of the library's built-in far-field scratch, used by h2b_farmul_noalloc. */
+#define H2B_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/*
+ * Far part without a workspace and without any device allocation.
+ *
+ * This entry point has no counterpart in the reference; it exists for callers that cannot
+ * allocate device memory at the time they multiply: a host whose device memory is owned by
+ * another allocator (a framework's caching pool that holds the GPU), a real-time loop that
+ * forbids allocation after start-up, or a binding that cannot create and keep a workspace.
+ * Instead of a workspace's moment and spectrum arenas it uses one scratch array compiled into
+ * the library (H2B_NOALLOC_SCRATCH_BYTES per device, held by every GPU that loads the library
+ * until the process exits). Same semantics as h2b_farmul on `core`.
+ *
+ * Limits and rules:
+ *   - the map's scratch for `nrhs` right-hand sides (two moment arenas, plus two spectrum arenas
+ *     for Toeplitz couplings) must fit in H2B_NOALLOC_SCRATCH_BYTES, else H2B_ERR_UNSUPPORTED;
+ *   - the first call on a device looks up the scratch array's device address for that device;
+ *     make that first call before any stream capture;
+ *   - all calls on a device share the one array: calls whose work overlaps on the GPU (other
+ *     streams, other host threads) race and corrupt each other's results. Serialise them.
+ *   - it allocates nothing: no cudaMalloc, no cudaFree, no allocating library routine.
+ */
+h2b_status h2b_farmul_noalloc(const h2b_core *core, int32_t mode, int32_t nrhs, const void *x,
+                              int64_t ldx, void *y, int64_t ldy, const double *alpha,
+                              const double *beta, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

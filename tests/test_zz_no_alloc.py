@@ -1,0 +1,105 @@
+"""h2b_farmul_noalloc: the far product for callers that cannot allocate device memory (GPU).
+
+Some hosts cannot call cudaMalloc when they multiply: their device memory is owned by another
+allocator (a framework's caching pool), or their serving loop forbids allocation after start-up.
+The entry point runs the far passes in a scratch array compiled into the library instead of a
+workspace. This file checks, through the C ABI, that it gives the same result as the workspace
+path (h2b_farmul) on two calls in a row -- the second call finds the first call's data in the
+shared scratch -- and that a map too large for the scratch is refused with a clear error.
+
+The file name sorts last so that a run stopping at the first failure has run every other test.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import h2factory_b200 as h2
+from h2factory_b200 import _abi, methods
+from h2factory_b200.trees import build_tree
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+TOL64 = 1e-12   # same bar as the FP64 parity tests
+TOL32 = 1e-5
+
+
+def _cols(a, dt):
+    a = np.asarray(a, dtype=dt)
+    return torch.from_numpy(np.ascontiguousarray(a.T)).to(DEV).t()
+
+
+def _noalloc(dcore, mode, x, y, alpha=None, beta=None):
+    lib = _abi.load_library()
+    n_in, nrhs = x.shape
+    ab = None
+    if alpha is not None:
+        a, b = complex(alpha), complex(beta)
+        ab = ((C.c_double * 2)(a.real, a.imag), (C.c_double * 2)(b.real, b.imag))
+    st = lib.h2b_farmul_noalloc(dcore.handle, mode, nrhs, C.c_void_p(x.data_ptr()), n_in,
+                                C.c_void_p(y.data_ptr()), y.shape[0], ab[0] if ab else None,
+                                ab[1] if ab else None,
+                                C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return st, lib.h2b_last_error().decode()
+
+
+def _maps():
+    rng = np.random.default_rng(3)
+    t = build_tree(rng.random((3000, 3)), depth=4, root_center=[0.5] * 3, root_halfsize=0.5)
+    yield "toeplitz-laplace", methods.interpolation_core(
+        t, methods.laplace, 3, nodes="equispaced", couplings="toeplitz"), TOL64
+    t2 = build_tree(rng.random((2000, 3)), maxvalues=40, root_center=[0.5] * 3, root_halfsize=0.5)
+    yield "chebyshev-helmholtz", methods.interpolation_core(t2, methods.helmholtz(3.0), 3), TOL64
+    core32 = methods.interpolation_core(t2, methods.helmholtz(3.0), 3, precision="fp32")
+    yield "chebyshev-helmholtz-fp32", core32, TOL32
+
+
+@pytest.mark.parametrize("name", ["toeplitz-laplace", "chebyshev-helmholtz", "chebyshev-helmholtz-fp32"])
+def test_noalloc_matches_workspace_farmul_twice(name):
+    core, tol = next((c, t) for n, c, t in _maps() if n == name)
+    ws = h2.H2Workspace(core, max_nrhs=3)
+    dt = core.dtype
+    rng = np.random.default_rng(7)
+    n = core.trial.npoints
+    for call in range(2):  # two calls in a row share (and reuse) the scratch
+        for mode, view in ((0, ws), (1, h2.transpose(ws)), (2, h2.adjoint(ws))):
+            xh = rng.standard_normal((n, 3))
+            if core.field == "complex":
+                xh = xh + 1j * rng.standard_normal((n, 3))
+            x = _cols(xh, dt)
+            want = _cols(np.zeros((n, 3)), dt)
+            h2.farmul_(want, view, x)
+            got = _cols(np.full((n, 3), np.nan), dt)
+            st, err = _noalloc(ws.dcore, mode, x, got)
+            assert st == 0, err
+            torch.cuda.synchronize()
+            w, g = want.cpu().numpy(), got.cpu().numpy()
+            assert np.linalg.norm(g - w) / np.linalg.norm(w) < tol, (name, call, mode)
+            # 5-argument form on a filled y
+            y0 = rng.standard_normal((n, 3)) + (1j * rng.standard_normal((n, 3)) if core.field == "complex" else 0)
+            want = _cols(y0, dt)
+            got = _cols(y0, dt)
+            a, b = (0.5 - 0.25j, 2.0 + 1.0j) if core.field == "complex" else (0.5, 2.0)
+            h2.farmul_(want, view, x, a, b)
+            st, err = _noalloc(ws.dcore, mode, x, got, a, b)
+            assert st == 0, err
+            torch.cuda.synchronize()
+            w, g = want.cpu().numpy(), got.cpu().numpy()
+            assert np.linalg.norm(g - w) / np.linalg.norm(w) < tol, (name, call, mode, "scaled")
+
+
+def test_noalloc_refuses_maps_beyond_the_scratch():
+    rng = np.random.default_rng(0)
+    t = build_tree(rng.random((8192, 3)), maxvalues=64, root_center=[0.5] * 3, root_halfsize=0.5)
+    core = methods.interpolation_core(t, methods.laplace, 4)
+    dcore = h2.DeviceCore(core)
+    per_rhs = 2 * dcore.info().moment_elems * 8
+    nrhs = _abi.H2B_NOALLOC_SCRATCH_BYTES // per_rhs + 2
+    x = torch.zeros((nrhs, 8192), dtype=torch.float64, device=DEV).t()
+    y = torch.zeros((nrhs, 8192), dtype=torch.float64, device=DEV).t()
+    st, err = _noalloc(dcore, 0, x, y)
+    assert st == _abi.H2B_ERR_UNSUPPORTED
+    assert "built-in scratch" in err
