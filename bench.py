@@ -356,7 +356,7 @@ def gpu_arm(args, rank, world, local_rank):
     near_ms = ntotal / len(nper)
     achieved = near_bytes / (near_ms * 1e-3) / 1e9
     workload = WORKLOAD if (args.n, args.depth) == (262144, 5) else f"toeplitz-laplace-N{args.n}-depth{args.depth}-p4"
-    traffic = traffic_table().get(("near_forward_kernel", workload))
+    traffic = traffic_table().get(("near_rows_kernel", workload))
     launches = sum(launches_per_step(core, i % 2) for i in range(args.steps))
     rhs_total = args.steps * nrhs * world
     line = {
@@ -373,7 +373,7 @@ def gpu_arm(args, rank, world, local_rank):
         "e2e": {"value": rhs_total / world / e2e_total, "unit": "RHS/s",
                 "h2d_bytes_per_step": int(n * 8 * nrhs), "d2h_bytes_per_step": int(n * 8 * nrhs),
                 "p50_ms": pct(te, 50) * 1e3, "p99_ms": pct(te, 99) * 1e3},
-        "roofline": {"kernel": "near_forward_kernel", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": "near_rows_kernel", "bound": "hbm", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                      "traffic": traffic, "algorithmic_bytes": near_bytes, "avg_launch_ms": near_ms},
         "clocks": clk.summary(),
@@ -395,7 +395,7 @@ def core_with_host_near(core, near_host):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nrhs", type=int, default=1)

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -89,7 +90,6 @@ struct h2b_core {
     DMap dmap{};
     DNear dnear{};
     SideHost test, trial;
-    int near_maxvals = 1;
     int64_t near_entries = 0;
     std::vector<void *> allocs;
     int64_t bytes = 0;
@@ -141,6 +141,11 @@ int64_t tsize_host(const h2b_side_desc &s, int lvl) {
            (2 * (int64_t)s.shape[3 * lvl + 2] - 1);
 }
 bool isleaf(const h2b_side_desc &s, int n) { return s.child_ptr[n + 1] == s.child_ptr[n]; }
+// stored spectrum length: the whole padded array, or its first-axis half for Hermitian spectra
+int64_t spec_len(const h2b_side_desc &s, int lvl, bool half) {
+    const int64_t t0 = 2 * (int64_t)s.shape[3 * lvl] - 1;
+    return half ? (t0 / 2 + 1) * (tsize_host(s, lvl) / t0) : tsize_host(s, lvl);
+}
 
 h2b_status validate_side(const h2b_map_desc &d, const h2b_side_desc &s, const h2b_side_desc &other,
                          const char *name) {
@@ -326,8 +331,9 @@ h2b_status validate(const h2b_map_desc &d) {
     if (d.coupling_kind == H2B_COUPLING_TOEPLITZ) {
         for (const h2b_side_desc *s : {&d.test, &d.trial})
             for (int l = 1; l <= s->nlevels; ++l)
-                if (tsize_host(*s, l) > 4096)
-                    return fail(H2B_ERR_UNSUPPORTED, "Toeplitz padded arrays above 4096 entries");
+                for (int k = 0; k < 3; ++k)
+                    if (s->shape[3 * l + k] > 8)
+                        return fail(H2B_ERR_UNSUPPORTED, "Toeplitz moments are limited to 8 points per axis");
     }
     // near blocks
     if (d.near_nrows < 0) return fail(H2B_ERR_INVALID, "near_nrows");
@@ -445,7 +451,7 @@ h2b_status build_side(h2b_core *c, const h2b_map_desc &d, const h2b_side_desc &s
         mo[n] = mt;
         so[n] = stot;
         mt += d.ncomp * ncoef_host(s, s.level[n]);
-        if (toep) stot += d.ncomp * tsize_host(s, s.level[n]);
+        if (toep) stot += d.ncomp * spec_len(s, s.level[n], c->dmap.half_spectrum != 0);
     }
     h.mom_total = mt;
     h.spec_total = stot;
@@ -518,22 +524,32 @@ h2b_status build_side(h2b_core *c, const h2b_map_desc &d, const h2b_side_desc &s
     return H2B_OK;
 }
 
+// Near blocks: repacked into the padded column-major layout of the near kernel (h2b_near.cu),
+// grouped by output leaf. N^T is needed for transpose/adjoint products: when the test and trial
+// sides are the same tree and every block equals the transpose of its mirror block (checked on the
+// device), N^T == N and N serves both; otherwise a transposed copy is built once here.
 h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
+    const bool cplx = d.field == H2B_COMPLEX;
+    const size_t vb = cplx ? 2 * sizeof(double) : sizeof(double);
     const int nb = d.near_nrows > 0 ? d.near_ptr[d.near_nrows] : 0;
     std::vector<int> blk_row(nb), blk_col(nb);
-    std::vector<int64_t> blk_off(nb);
-    int64_t entries = 0;
+    std::vector<int64_t> src_off(nb), fwd_off(nb), tr_off(nb);
+    int64_t entries = 0, fwd_len = 0, tr_len = 0;
+    auto nv = [](const h2b_side_desc &s, int n) { return s.value_ptr[n + 1] - s.value_ptr[n]; };
     for (int g = 0; g < d.near_nrows; ++g)
         for (int b = d.near_ptr[g]; b < d.near_ptr[g + 1]; ++b) {
             blk_row[b] = d.near_row[g];
             blk_col[b] = d.near_col[b];
-            blk_off[b] = d.near_offset[b];
-            const int64_t nr = d.test.value_ptr[blk_row[b] + 1] - d.test.value_ptr[blk_row[b]];
-            const int64_t nc = d.trial.value_ptr[blk_col[b] + 1] - d.trial.value_ptr[blk_col[b]];
-            entries += nr * nc;
+            src_off[b] = d.near_offset[b];
+            const int nr = nv(d.test, blk_row[b]), nc = nv(d.trial, blk_col[b]);
+            entries += (int64_t)nr * nc;
+            fwd_off[b] = fwd_len;
+            fwd_len += near_padded_ld(cplx, nr) * nc;
+            tr_off[b] = tr_len;
+            tr_len += near_padded_ld(cplx, nc) * nr;
         }
     c->near_entries = entries;
-    // groups over every leaf, so that leaves without near blocks still get y = beta * y
+    // groups over every output leaf, so that leaves without near blocks still get y = beta * y
     auto groups = [&](const h2b_side_desc &s, const std::vector<int> &key, std::vector<int> &leaf,
                       std::vector<int> &ptr, std::vector<int> &blk) {
         std::vector<int> slot(s.nnodes, -1);
@@ -542,60 +558,179 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
         ptr.assign(leaf.size() + 1, 0);
         for (int b = 0; b < nb; ++b) ptr[slot[key[b]] + 1]++;
         for (size_t g = 0; g < leaf.size(); ++g) ptr[g + 1] += ptr[g];
-        blk.assign(nb, 0);
+        blk.assign(std::max(nb, 1), 0);
         std::vector<int> fill(ptr.begin(), ptr.end() - 1);
         for (int b = 0; b < nb; ++b) blk[fill[slot[key[b]]]++] = b;
     };
-    std::vector<int> rl, rp, rb, cl, cp, cb;
-    groups(d.test, blk_row, rl, rp, rb);
-    groups(d.trial, blk_col, cl, cp, cb);
-    DNear &N = c->dnear;
     int *p;
-    CUDA_TRY(c->upload(&p, rl.data(), rl.size())); N.row_leaf = p;
-    CUDA_TRY(c->upload(&p, rp.data(), rp.size())); N.row_ptr = p;
-    CUDA_TRY(c->upload(&p, rb.data(), rb.size())); N.row_blk = p;
-    CUDA_TRY(c->upload(&p, cl.data(), cl.size())); N.col_leaf = p;
-    CUDA_TRY(c->upload(&p, cp.data(), cp.size())); N.col_ptr = p;
-    CUDA_TRY(c->upload(&p, cb.data(), cb.size())); N.col_blk = p;
-    CUDA_TRY(c->upload(&p, blk_row.data(), blk_row.size())); N.blk_row = p;
-    CUDA_TRY(c->upload(&p, blk_col.data(), blk_col.size())); N.blk_col = p;
     int64_t *q;
-    CUDA_TRY(c->upload(&q, blk_off.data(), blk_off.size())); N.blk_off = q;
-    N.nrow_groups = (int)rl.size();
-    N.ncol_groups = (int)cl.size();
-    const size_t vb = d.field == H2B_COMPLEX ? 2 * sizeof(double) : sizeof(double);
-    void *data = nullptr;
-    const size_t bytes = (size_t)std::max<int64_t>(d.near_len, 1) * vb;
-    CUDA_TRY(cudaMalloc(&data, bytes));
-    c->allocs.push_back(data);
-    c->bytes += (int64_t)bytes;
-    if (d.near_len > 0)
-        CUDA_TRY(cudaMemcpy(data, d.near, (size_t)d.near_len * vb,
-                            d.near_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
-    N.data = data;
-    c->near_maxvals = std::max(c->test.maxvals, c->trial.maxvals);
+    int *d_row, *d_col;
+    int64_t *d_src_off;
+    CUDA_TRY(c->upload(&d_row, blk_row.data(), blk_row.size()));
+    CUDA_TRY(c->upload(&d_col, blk_col.data(), blk_col.size()));
+    CUDA_TRY(c->upload(&d_src_off, src_off.data(), src_off.size()));
+
+    // source blocks on the device (the caller's device buffer, or a temporary upload)
+    const void *src = d.near;
+    void *tmp = nullptr;
+    if (!d.near_on_device && d.near_len > 0) {
+        CUDA_TRY(cudaMalloc(&tmp, (size_t)d.near_len * vb));
+        cudaError_t e = cudaMemcpy(tmp, d.near, (size_t)d.near_len * vb, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(tmp);
+            return fail(H2B_ERR_CUDA, "near upload failed: %s", cudaGetErrorString(e));
+        }
+        src = tmp;
+    }
+    struct TmpGuard {
+        void *p;
+        ~TmpGuard() { if (p) cudaFree(p); }
+    } tguard{tmp};
+
+    // N in the padded layout, grouped by test leaf
+    {
+        std::vector<int> leaf, ptr, blk;
+        groups(d.test, blk_row, leaf, ptr, blk);
+        NearOp &op = c->dnear.fwd;
+        CUDA_TRY(c->upload(&p, leaf.data(), leaf.size())); op.grp_leaf = p;
+        CUDA_TRY(c->upload(&p, ptr.data(), ptr.size())); op.grp_ptr = p;
+        CUDA_TRY(c->upload(&p, blk.data(), blk.size())); op.grp_blk = p;
+        op.blk_in = d_col;
+        CUDA_TRY(c->upload(&q, fwd_off.data(), fwd_off.size())); op.blk_off = q;
+        unsigned char *data;
+        CUDA_TRY(c->alloc(&data, (size_t)std::max<int64_t>(fwd_len, 2) * vb));
+        op.data = data;
+        op.ngroups = (int)leaf.size();
+        if (nb > 0)
+            CUDA_TRY(launch_near_repack(cplx, src, d_src_off, d_row, d_col, c->test.d, c->trial.d, data,
+                                        op.blk_off, nb, false, 0));
+    }
+
+    // N^T == N ?
+    bool symmetric = false;
+    const bool same_tree = d.test.nnodes == d.trial.nnodes && d.test.ndofs == d.trial.ndofs &&
+                           std::equal(d.test.value_ptr, d.test.value_ptr + d.test.nnodes + 1, d.trial.value_ptr) &&
+                           std::equal(d.test.value, d.test.value + d.test.value_ptr[d.test.nnodes], d.trial.value);
+    if (same_tree) {
+        std::vector<int> mirror(std::max(nb, 1), -1);
+        std::vector<int64_t> key(nb);
+        std::vector<int> order(nb);
+        for (int b = 0; b < nb; ++b) {
+            key[b] = (int64_t)blk_row[b] * d.test.nnodes + blk_col[b];
+            order[b] = b;
+        }
+        std::sort(order.begin(), order.end(), [&](int a, int b2) { return key[a] < key[b2]; });
+        bool all = true;
+        for (int b = 0; b < nb && all; ++b) {
+            const int64_t want = (int64_t)blk_col[b] * d.test.nnodes + blk_row[b];
+            auto it = std::lower_bound(order.begin(), order.end(), want,
+                                       [&](int a, int64_t v) { return key[a] < v; });
+            if (it == order.end() || key[*it] != want) all = false;
+            else mirror[b] = *it;
+        }
+        if (all) {
+            int *d_mirror, *d_flag;
+            CUDA_TRY(c->upload(&d_mirror, mirror.data(), mirror.size()));
+            const int one = 1;
+            CUDA_TRY(c->upload(&d_flag, &one, 1));
+            CUDA_TRY(launch_near_symcheck(cplx, src, d_src_off, d_mirror, d_row, c->test.d, nb, d_flag, 0));
+            int flag = 0;
+            CUDA_TRY(cudaMemcpy(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+            symmetric = flag == 1;
+        }
+    }
+    c->dnear.symmetric = symmetric;
+
+    if (!symmetric) {
+        // N^T in the padded layout, grouped by trial leaf
+        std::vector<int> leaf, ptr, blk;
+        groups(d.trial, blk_col, leaf, ptr, blk);
+        NearOp &op = c->dnear.tr;
+        CUDA_TRY(c->upload(&p, leaf.data(), leaf.size())); op.grp_leaf = p;
+        CUDA_TRY(c->upload(&p, ptr.data(), ptr.size())); op.grp_ptr = p;
+        CUDA_TRY(c->upload(&p, blk.data(), blk.size())); op.grp_blk = p;
+        op.blk_in = d_row;
+        CUDA_TRY(c->upload(&q, tr_off.data(), tr_off.size())); op.blk_off = q;
+        unsigned char *data;
+        CUDA_TRY(c->alloc(&data, (size_t)std::max<int64_t>(tr_len, 2) * vb));
+        op.data = data;
+        op.ngroups = (int)leaf.size();
+        if (nb > 0)
+            CUDA_TRY(launch_near_repack(cplx, src, d_src_off, d_row, d_col, c->test.d, c->trial.d, data,
+                                        op.blk_off, nb, true, 0));
+    }
+    CUDA_TRY(cudaDeviceSynchronize());
     return H2B_OK;
 }
 
+// Padded shape (2s - 1 per axis) of every coupling, from the pairs that use it; 0 if unused.
+std::vector<int> coupling_shapes(const h2b_map_desc &d) {
+    std::vector<int> ts(3 * std::max<int64_t>(d.ncouplings, 1), 0);
+    for (const h2b_side_desc *s : {&d.test, &d.trial})
+        for (int n = 0; n < s->nnodes; ++n)
+            for (int p = s->i2o_ptr[n]; p < s->i2o_ptr[n + 1]; ++p)
+                for (int k = 0; k < 3; ++k) ts[3 * s->i2o_coupling[p] + k] = 2 * s->shape[3 * s->level[n] + k] - 1;
+    return ts;
+}
+
+// Is every used Toeplitz coupling Hermitian, K[k] == conj(K[-k]) to rounding?
+bool couplings_hermitian(const h2b_map_desc &d, const std::vector<int> &ts) {
+    for (int64_t c = 0; c < d.ncouplings; ++c) {
+        const int n0 = ts[3 * c], n1 = ts[3 * c + 1], n2 = ts[3 * c + 2];
+        if (n0 == 0) continue;
+        const double *K = d.coupling + d.coupling_offset[c];
+        double mx = 0.0;
+        for (int64_t e = 0; e < (int64_t)n0 * n1 * n2; ++e) mx = std::max(mx, std::hypot(K[2 * e], K[2 * e + 1]));
+        const double tol = 1e-12 * std::max(mx, 1e-300);
+        for (int k3 = 0; k3 < n2; ++k3)
+            for (int k2 = 0; k2 < n1; ++k2)
+                for (int k1 = 0; k1 < n0; ++k1) {
+                    const int64_t e = k1 + (int64_t)n0 * (k2 + (int64_t)n1 * k3);
+                    const int64_t f = (n0 - k1) % n0 + (int64_t)n0 * ((n1 - k2) % n1 + (int64_t)n1 * ((n2 - k3) % n2));
+                    if (std::fabs(K[2 * e] - K[2 * f]) > tol || std::fabs(K[2 * e + 1] + K[2 * f + 1]) > tol)
+                        return false;
+                }
+    }
+    return true;
+}
+
 h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
-    h2b_status st = build_side(c, d, d.test, d.trial, c->test);
-    if (st) return st;
-    st = build_side(c, d, d.trial, d.test, c->trial);
-    if (st) return st;
     DMap &M = c->dmap;
     M.ncomp = d.ncomp;
     M.dim = d.dim;
     M.nsectors = d.nsectors;
     M.transfer_kind = d.transfer_kind;
     M.coupling_kind = d.coupling_kind;
+    const bool cplx = d.field == H2B_COMPLEX;
+    const bool toep = d.coupling_kind == H2B_COUPLING_TOEPLITZ;
+    std::vector<int> ts;
+    if (toep) ts = coupling_shapes(d);
+    M.half_spectrum = toep && !cplx && couplings_hermitian(d, ts);
+    h2b_status st = build_side(c, d, d.test, d.trial, c->test);
+    if (st) return st;
+    st = build_side(c, d, d.trial, d.test, c->trial);
+    if (st) return st;
     // coupling data: offsets arrive in doubles; convert to elements of the device type
     std::vector<int64_t> off(std::max<int64_t>(d.ncouplings, 1), 0);
-    const bool cplx = d.field == H2B_COMPLEX;
-    if (d.coupling_kind == H2B_COUPLING_TOEPLITZ) {
-        for (int64_t k = 0; k < d.ncouplings; ++k) off[k] = d.coupling_offset[k] / 2;
-        const int64_t n = d.coupling_len / 2;
-        if (c->precision == H2B_FP64) st = upload_scalars<cdouble>(c, d.coupling, n, &M.cpl);
-        else st = upload_scalars<cfloat>(c, d.coupling, n, &M.cpl);
+    if (toep) {
+        // spectra as stored: whole padded arrays, or their first-axis halves
+        std::vector<double> packed;
+        for (int64_t k = 0; k < d.ncouplings; ++k) {
+            off[k] = (int64_t)packed.size() / 2;
+            const int n0 = ts[3 * k], n1 = ts[3 * k + 1], n2 = ts[3 * k + 2];
+            if (n0 == 0) continue;
+            const int h0 = M.half_spectrum ? n0 / 2 + 1 : n0;
+            const double *K = d.coupling + d.coupling_offset[k];
+            for (int r = 0; r < n1 * n2; ++r)
+                for (int k1 = 0; k1 < h0; ++k1) {
+                    packed.push_back(K[2 * (k1 + (int64_t)n0 * r)]);
+                    packed.push_back(K[2 * (k1 + (int64_t)n0 * r) + 1]);
+                }
+        }
+        if (packed.empty()) packed.assign(2, 0.0);
+        const int64_t n = (int64_t)packed.size() / 2;
+        if (c->precision == H2B_FP64) st = upload_scalars<cdouble>(c, packed.data(), n, &M.cpl);
+        else st = upload_scalars<cfloat>(c, packed.data(), n, &M.cpl);
     } else {
         const int fw = cplx ? 2 : 1;
         for (int64_t k = 0; k < d.ncouplings; ++k) off[k] = d.coupling_offset[k] / fw;
@@ -808,8 +943,7 @@ h2b_status run(h2b_workspace *ws, Kind kind, int32_t mode, int32_t nrhs, const v
     const SideHost &cols = c->trial;
     h2b_status s = H2B_OK;
     if (kind == KIND_NEAR) {
-        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b,
-                             c->near_maxvals, st));
+        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b, st));
     } else if (kind == KIND_FAR) {
         if (!alpha) {
             CUDA_TRY(launch_zero_columns(cplx, nrhs, nout, y, ldy, st));
@@ -821,8 +955,7 @@ h2b_status run(h2b_workspace *ws, Kind kind, int32_t mode, int32_t nrhs, const v
         // near on the auxiliary stream, far on the caller's; the leaf scatter waits for the near
         CUDA_TRY(cudaEventRecord(ws->ev_fork, st));
         CUDA_TRY(cudaStreamWaitEvent(ws->aux, ws->ev_fork, 0));
-        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b,
-                             c->near_maxvals, ws->aux));
+        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b, ws->aux));
         CUDA_TRY(cudaEventRecord(ws->ev_join, ws->aux));
         s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(aA, a), cdouble{1.0, 0.0}, st, ws->ev_join);
     }

@@ -81,23 +81,27 @@ struct DSide {
 struct DMap {
     int ncomp, dim, nsectors;
     int transfer_kind, coupling_kind;
+    int half_spectrum;       // Toeplitz spectra stored as half spectra (real maps, Hermitian couplings)
     const int64_t *cpl_off;  // [ncouplings] offsets in elements of T (dense/diag) or spectrum (Toeplitz)
     const void *cpl;
 };
 
-// Near blocks in block-CSR by test leaf (forward) and block-CSC by trial leaf (transposed).
+// One oriented near operator: for every output leaf (group), the dense blocks that write its rows.
+// Blocks are column-major, output rows x input columns, leading dimension near_padded_ld(rows).
+struct NearOp {
+    int ngroups = 0;
+    const int *grp_leaf = nullptr;  // [ngroups] output leaf (every output leaf has a group)
+    const int *grp_ptr = nullptr;   // [ngroups+1]
+    const int *grp_blk = nullptr;   // block ids
+    const int *blk_in = nullptr;    // input leaf of each block
+    const int64_t *blk_off = nullptr;
+    const void *data = nullptr;     // V
+};
+
 struct DNear {
-    const int *row_leaf;   // [nrow_groups] test leaf of each group (covers every test leaf)
-    const int *row_ptr;    // [nrow_groups+1]
-    const int *row_blk;    // block ids
-    const int *col_leaf;   // [ncol_groups] trial leaf of each group (covers every trial leaf)
-    const int *col_ptr;
-    const int *col_blk;
-    const int *blk_row;    // [nblocks] test leaf of block
-    const int *blk_col;    // [nblocks] trial leaf of block
-    const int64_t *blk_off;
-    const void *data;      // V
-    int nrow_groups, ncol_groups;
+    NearOp fwd;              // N: rows on the test side, columns on the trial side
+    NearOp tr;               // N^T (unused when symmetric)
+    bool symmetric = false;  // N^T == N: transposed products run on `fwd`
 };
 
 // Per-call arguments of the far passes.
@@ -136,9 +140,16 @@ cudaError_t launch_leaf_disaggregate(bool cplx, int precision, const DMap &m, co
                                      const int *leaves, int nleaves, bool conjc, const FarArgs &fa,
                                      cdouble alpha, cdouble beta, void *y, int64_t ldy,
                                      cudaStream_t st);
-cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &rows,
-                        const DSide &cols, int nrhs, const void *x, int64_t ldx, void *y,
-                        int64_t ldy, cdouble alpha, cdouble beta, int maxvals, cudaStream_t st);
+cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &test, const DSide &trial,
+                        int nrhs, const void *x, int64_t ldx, void *y, int64_t ldy, cdouble alpha,
+                        cdouble beta, cudaStream_t st);
+int64_t near_padded_ld(bool cplx, int n);
+cudaError_t launch_near_repack(bool cplx, const void *src, const int64_t *src_off, const int *blk_row,
+                               const int *blk_col, const DSide &rows, const DSide &cols, void *dst,
+                               const int64_t *dst_off, int nblocks, bool transpose, cudaStream_t st);
+cudaError_t launch_near_symcheck(bool cplx, const void *src, const int64_t *off, const int *mirror,
+                                 const int *blk_row, const DSide &rows, int nblocks, int *flag,
+                                 cudaStream_t st);
 cudaError_t launch_zero_columns(bool cplx, int nrhs, int64_t n, void *y, int64_t ldy,
                                 cudaStream_t st);
 

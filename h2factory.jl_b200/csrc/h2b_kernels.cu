@@ -9,7 +9,7 @@
 //   toeplitz_out       B3  modulate_out!       toeplitzmul.jl:299-315
 //   transfer_down      C1  O2O                 src/farinteractions/disaggregation.jl:244-271
 //   leaf_disaggregate  C2  disaggregateleaf!   traversalhelpers.jl:84-96
-//   near_*             D   nearmul!            src/nearinteractions/nearmul.jl:8-14
+//   (near field: h2b_near.cu)
 // Column-major operands are read along their contiguous dimension by consecutive threads
 // (thread per row for A x), or by the lanes of one warp with a shuffle reduction (warp per
 // output for A^T x), so every global read is coalesced.
@@ -160,16 +160,34 @@ __global__ void transfer_up_kernel(DMap m, DSide s, const int *__restrict__ node
     const int c0 = s.child_ptr[p], c1 = s.child_ptr[p + 1];
     const int nq = m.ncomp * nrhs;
     if (m.transfer_kind == H2B_TRANSFER_DENSE) {
+        // children split over `ns` thread groups of `npad` threads, partial sums reduced in smem
+        const int npad = ((nout + 31) / 32) * 32;
+        const int ns = npad <= (int)blockDim.x ? (int)blockDim.x / npad : 1;
+        const int sidx = threadIdx.x / npad;
         for (int q = 0; q < nq; ++q)
-            for (int a = threadIdx.x; a < nout; a += blockDim.x) {
+            for (int a0 = 0; a0 < nout; a0 += (ns > 1 ? npad : (int)blockDim.x)) {
+                const int a = a0 + (ns > 1 ? (int)threadIdx.x % npad : (int)threadIdx.x);
                 T acc = sc_zero<T>();
-                for (int k = c0; k < c1; ++k) {
-                    const int ch = s.child[k];
-                    const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
-                    const T *mc = am + s.mom_off[ch] * nrhs + (int64_t)q * nin;
-                    for (int b = 0; b < nin; ++b) acc = acc + cj(Tk[a + (int64_t)b * nout], conjt) * mc[b];
+                if (sidx < ns && a < nout)
+                    for (int k = c0 + sidx; k < c1; k += ns) {
+                        const int ch = s.child[k];
+                        const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
+                        const T *mc = am + s.mom_off[ch] * nrhs + (int64_t)q * nin;
+#pragma unroll 4
+                        for (int b = 0; b < nin; ++b) acc = acc + cj(Tk[a + (int64_t)b * nout], conjt) * mc[b];
+                    }
+                if (ns > 1) {
+                    if (sidx < ns) sm[sidx * npad + (threadIdx.x % npad)] = acc;
+                    __syncthreads();
+                    if (threadIdx.x < npad && a0 + threadIdx.x < nout) {
+                        T sum = sm[threadIdx.x];
+                        for (int w = 1; w < ns; ++w) sum = sum + sm[w * npad + threadIdx.x];
+                        mp[(int64_t)q * nout + a0 + threadIdx.x] = sum;
+                    }
+                    __syncthreads();
+                } else if (a < nout) {
+                    mp[(int64_t)q * nout + a] = acc;
                 }
-                mp[(int64_t)q * nout + a] = acc;
             }
         return;
     }
@@ -191,96 +209,189 @@ __global__ void transfer_up_kernel(DMap m, DSide s, const int *__restrict__ node
 }
 
 // ---------------------------------------------------------------------------------------------
-// Multidimensional DFT of a column-major complex array in shared memory (AbstractFFTs
-// conventions: forward e^{-2 pi i jk/n}; inverse e^{+2 pi i jk/n} and 1/n per axis).
+// Toeplitz transforms (modulate_in! / modulate_out!, src/moments/toeplitz/toeplitzmul.jl:290-315).
+// Several transforms per CTA, FFT_T threads each, in shared memory. A multidimensional DFT is one
+// pass per axis; in a pass each thread owns whole lines along that axis, holds a line in
+// registers and writes the transformed line back in place. AbstractFFTs conventions: forward
+// e^{-2 pi i jk/n}; inverse e^{+2 pi i jk/n} with 1/n per axis. Axes are at most FFT_NMAX long.
+// With `half` set (real maps), only the first n/2 + 1 entries along the first axis are stored; the
+// rest follow from Hermitian symmetry S[k] = conj(S[-k]).
 // ---------------------------------------------------------------------------------------------
+constexpr int FFT_T = 64;
+constexpr int FFT_NMAX = 16;
+
+struct TGeom {
+    int ts[3];   // padded extents 2s - 1
+    int sh[3];   // moment extents s
+    int nt, nc;  // padded / moment sizes
+    int h0;      // stored extent along the first axis (half or full)
+    int slen;    // stored spectrum length
+};
+
+__device__ __forceinline__ TGeom tgeom(const DSide &s, int lvl, bool half) {
+    TGeom g;
+    for (int d = 0; d < 3; ++d) {
+        g.sh[d] = s.shape[3 * lvl + d];
+        g.ts[d] = 2 * g.sh[d] - 1;
+    }
+    g.nt = g.ts[0] * g.ts[1] * g.ts[2];
+    g.nc = g.sh[0] * g.sh[1] * g.sh[2];
+    g.h0 = half ? g.ts[0] / 2 + 1 : g.ts[0];
+    g.slen = g.h0 * g.ts[1] * g.ts[2];
+    return g;
+}
+
+template <class R, int N>
+__device__ __forceinline__ void dft_line(Cx<R> *a, int base, int stride, const Cx<R> *tw, R scale) {
+    Cx<R> v[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) v[j] = a[base + j * stride];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        Cx<R> acc = v[0];
+#pragma unroll
+        for (int j = 1; j < N; ++j) acc = acc + v[j] * tw[(j * k) % N];
+        a[base + k * stride] = scale * acc;
+    }
+}
+
 template <class R>
-__device__ void dft_block(Cx<R> *&a, Cx<R> *&b, const int *ts, bool inverse, Cx<R> *tw) {
-    const int total = ts[0] * ts[1] * ts[2];
-    for (int ax = 0; ax < 3; ++ax) {
-        const int n = ts[ax];
-        if (n == 1) continue;
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            double sv, cv;
-            sincospi(2.0 * k / n, &sv, &cv);
-            tw[k] = {(R)cv, (R)(inverse ? sv : -sv)};
-        }
-        __syncthreads();
-        const int stride = ax == 0 ? 1 : (ax == 1 ? ts[0] : ts[0] * ts[1]);
-        const R scale = inverse ? (R)1 / (R)n : (R)1;
-        for (int e = threadIdx.x; e < total; e += blockDim.x) {
-            const int k = (e / stride) % n;
-            const int base = e - k * stride;
-            Cx<R> acc = {(R)0, (R)0};
-            int w = 0;
-            for (int j = 0; j < n; ++j) {
-                acc = acc + a[base + j * stride] * tw[w];
-                w += k;
-                if (w >= n) w -= n;
+__device__ __forceinline__ void dft_line_n(int n, Cx<R> *a, int base, int stride, const Cx<R> *tw, R scale) {
+    switch (n) {
+    case 2: dft_line<R, 2>(a, base, stride, tw, scale); break;
+    case 3: dft_line<R, 3>(a, base, stride, tw, scale); break;
+    case 4: dft_line<R, 4>(a, base, stride, tw, scale); break;
+    case 5: dft_line<R, 5>(a, base, stride, tw, scale); break;
+    case 6: dft_line<R, 6>(a, base, stride, tw, scale); break;
+    case 7: dft_line<R, 7>(a, base, stride, tw, scale); break;
+    case 8: dft_line<R, 8>(a, base, stride, tw, scale); break;
+    case 9: dft_line<R, 9>(a, base, stride, tw, scale); break;
+    case 10: dft_line<R, 10>(a, base, stride, tw, scale); break;
+    case 11: dft_line<R, 11>(a, base, stride, tw, scale); break;
+    case 12: dft_line<R, 12>(a, base, stride, tw, scale); break;
+    case 13: dft_line<R, 13>(a, base, stride, tw, scale); break;
+    case 14: dft_line<R, 14>(a, base, stride, tw, scale); break;
+    case 15: dft_line<R, 15>(a, base, stride, tw, scale); break;
+    case 16: dft_line<R, 16>(a, base, stride, tw, scale); break;
+    default: break;
+    }
+}
+
+// In-place multidimensional DFT of one transform held by FFT_T threads (tl = thread in group).
+// Every thread of the CTA calls this the same number of times (3 barriers), busy or not.
+template <class R>
+__device__ void dft_group(Cx<R> *a, const TGeom &g, bool inverse, Cx<R> *tw, int tl, bool busy) {
+    // twiddles of the three axes: tw[16 * ax + k] = e^{-+2 pi i k / n}
+    if (busy)
+        for (int e = tl; e < 3 * FFT_NMAX; e += FFT_T) {
+            const int ax = e / FFT_NMAX, k = e % FFT_NMAX;
+            const int n = g.ts[ax];
+            if (k < n) {
+                double sv, cv;
+                sincospi(2.0 * k / n, &sv, &cv);
+                tw[e] = {(R)cv, (R)(inverse ? sv : -sv)};
             }
-            b[e] = scale * acc;
+        }
+    __syncthreads();
+    for (int ax = 0; ax < 3; ++ax) {
+        const int n = g.ts[ax];
+        if (busy && n > 1) {
+            const int nlines = g.nt / n;
+            const R scale = inverse ? (R)1 / (R)n : (R)1;
+            for (int l = tl; l < nlines; l += FFT_T) {
+                int base, stride;
+                if (ax == 0) {
+                    base = l * n;
+                    stride = 1;
+                } else if (ax == 1) {
+                    base = (l % g.ts[0]) + g.ts[0] * g.ts[1] * (l / g.ts[0]);
+                    stride = g.ts[0];
+                } else {
+                    base = l;
+                    stride = g.ts[0] * g.ts[1];
+                }
+                dft_line_n(n, a, base, stride, tw + FFT_NMAX * ax, scale);
+            }
         }
         __syncthreads();
-        Cx<R> *t = a; a = b; b = t;
     }
 }
 
 // A3: spectrum(node) = F(pad(moment(node)))   (F = fft, or ifft for transpose maps)
 template <class T>
-__global__ void toeplitz_in_kernel(DMap m, DSide s, const int *__restrict__ nodes, bool inverse,
-                                   int nrhs, const T *__restrict__ am,
+__global__ void toeplitz_in_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
+                                   int nrhs, int maxt, const T *__restrict__ am,
                                    typename ScalarTraits<T>::Complex *__restrict__ as) {
     using S = typename ScalarTraits<T>::Complex;
+    using R = typename ScalarTraits<T>::Real;
     extern __shared__ unsigned char smem_raw[];
-    const int node = nodes[blockIdx.x];
-    const int lvl = s.level[node];
-    const int *sh = &s.shape[3 * lvl];
-    int ts[3] = {2 * sh[0] - 1, 2 * sh[1] - 1, 2 * sh[2] - 1};
-    const int nt = ts[0] * ts[1] * ts[2], nc = sh[0] * sh[1] * sh[2];
-    S *a = reinterpret_cast<S *>(smem_raw), *b = a + nt, *tw = b + nt;
-    const T *mom = am + s.mom_off[node] * nrhs;
-    S *spec = as + s.spec_off[node] * nrhs;
-    for (int q = 0; q < m.ncomp * nrhs; ++q) {
-        S *pa = a, *pb = b;
-        for (int e = threadIdx.x; e < nt; e += blockDim.x) {
-            const int i1 = e % ts[0], i2 = (e / ts[0]) % ts[1], i3 = e / (ts[0] * ts[1]);
-            S v = {0, 0};
-            if (i1 < sh[0] && i2 < sh[1] && i3 < sh[2])
-                v = to_cx(mom[(int64_t)q * nc + i1 + sh[0] * (i2 + sh[1] * i3)]);
-            pa[e] = v;
+    const int grp = threadIdx.x / FFT_T, tl = threadIdx.x % FFT_T, ngrp = blockDim.x / FFT_T;
+    S *a = reinterpret_cast<S *>(smem_raw) + (size_t)grp * (maxt + 3 * FFT_NMAX);
+    S *tw = a + maxt;
+    const int nq = m.ncomp * nrhs;
+    const int t = blockIdx.x * ngrp + grp;
+    const bool busy = t < ntrans;
+    const int node = busy ? nodes[t / nq] : nodes[0];
+    const int q = busy ? t % nq : 0;
+    const TGeom g = tgeom(s, s.level[node], m.half_spectrum != 0);
+    if (busy) {
+        const T *mom = am + s.mom_off[node] * nrhs + (int64_t)q * g.nc;
+        for (int e = tl; e < g.nt; e += FFT_T) {
+            const int i1 = e % g.ts[0], i2 = (e / g.ts[0]) % g.ts[1], i3 = e / (g.ts[0] * g.ts[1]);
+            S v = {(R)0, (R)0};
+            if (i1 < g.sh[0] && i2 < g.sh[1] && i3 < g.sh[2])
+                v = to_cx(mom[i1 + g.sh[0] * (i2 + g.sh[1] * i3)]);
+            a[e] = v;
         }
-        __syncthreads();
-        dft_block(pa, pb, ts, inverse, tw);
-        for (int e = threadIdx.x; e < nt; e += blockDim.x) spec[(int64_t)q * nt + e] = pa[e];
-        __syncthreads();
+    }
+    dft_group<R>(a, g, inverse, tw, tl, busy);
+    if (busy) {
+        S *spec = as + s.spec_off[node] * nrhs + (int64_t)q * g.slen;
+        for (int e = tl; e < g.slen; e += FFT_T) {
+            const int k1 = e % g.h0, r = e / g.h0;
+            spec[e] = a[k1 + g.ts[0] * r];
+        }
     }
 }
 
 // B3: moment(node) = corner(F^-1(spectrum(node)))   (overwrite)
 template <class T>
-__global__ void toeplitz_out_kernel(DMap m, DSide s, const int *__restrict__ nodes, bool inverse,
-                                    int nrhs, const typename ScalarTraits<T>::Complex *__restrict__ ds,
+__global__ void toeplitz_out_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
+                                    int nrhs, int maxt,
+                                    const typename ScalarTraits<T>::Complex *__restrict__ ds,
                                     T *__restrict__ dm) {
     using S = typename ScalarTraits<T>::Complex;
+    using R = typename ScalarTraits<T>::Real;
     extern __shared__ unsigned char smem_raw[];
-    const int node = nodes[blockIdx.x];
-    const int lvl = s.level[node];
-    const int *sh = &s.shape[3 * lvl];
-    int ts[3] = {2 * sh[0] - 1, 2 * sh[1] - 1, 2 * sh[2] - 1};
-    const int nt = ts[0] * ts[1] * ts[2], nc = sh[0] * sh[1] * sh[2];
-    S *a = reinterpret_cast<S *>(smem_raw), *b = a + nt, *tw = b + nt;
-    T *mom = dm + s.mom_off[node] * nrhs;
-    const S *spec = ds + s.spec_off[node] * nrhs;
-    for (int q = 0; q < m.ncomp * nrhs; ++q) {
-        S *pa = a, *pb = b;
-        for (int e = threadIdx.x; e < nt; e += blockDim.x) pa[e] = spec[(int64_t)q * nt + e];
-        __syncthreads();
-        dft_block(pa, pb, ts, inverse, tw);
-        for (int e = threadIdx.x; e < nc; e += blockDim.x) {
-            const int i1 = e % sh[0], i2 = (e / sh[0]) % sh[1], i3 = e / (sh[0] * sh[1]);
-            from_cx(pa[i1 + ts[0] * (i2 + ts[1] * i3)], mom[(int64_t)q * nc + e]);
+    const int grp = threadIdx.x / FFT_T, tl = threadIdx.x % FFT_T, ngrp = blockDim.x / FFT_T;
+    S *a = reinterpret_cast<S *>(smem_raw) + (size_t)grp * (maxt + 3 * FFT_NMAX);
+    S *tw = a + maxt;
+    const int nq = m.ncomp * nrhs;
+    const int t = blockIdx.x * ngrp + grp;
+    const bool busy = t < ntrans;
+    const int node = busy ? nodes[t / nq] : nodes[0];
+    const int q = busy ? t % nq : 0;
+    const TGeom g = tgeom(s, s.level[node], m.half_spectrum != 0);
+    if (busy) {
+        const S *spec = ds + s.spec_off[node] * nrhs + (int64_t)q * g.slen;
+        for (int e = tl; e < g.nt; e += FFT_T) {
+            const int k1 = e % g.ts[0], r = e / g.ts[0];
+            if (k1 < g.h0) {
+                a[e] = spec[k1 + g.h0 * r];
+            } else {
+                const int k2 = r % g.ts[1], k3 = r / g.ts[1];
+                const int m1 = g.ts[0] - k1, m2 = (g.ts[1] - k2) % g.ts[1], m3 = (g.ts[2] - k3) % g.ts[2];
+                a[e] = conjg(spec[m1 + g.h0 * (m2 + g.ts[1] * m3)]);
+            }
         }
-        __syncthreads();
+    }
+    dft_group<R>(a, g, inverse, tw, tl, busy);
+    if (busy) {
+        T *mom = dm + s.mom_off[node] * nrhs + (int64_t)q * g.nc;
+        for (int e = tl; e < g.nc; e += FFT_T) {
+            const int i1 = e % g.sh[0], i2 = (e / g.sh[0]) % g.sh[1], i3 = e / (g.sh[0] * g.sh[1]);
+            from_cx(a[i1 + g.ts[0] * (i2 + g.ts[1] * i3)], mom[e]);
+        }
     }
 }
 
@@ -303,13 +414,13 @@ __global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nod
     const int nq = m.ncomp * nrhs;
     const bool adj = (mode == H2B_ADJOINT);
     if (m.coupling_kind == H2B_COUPLING_TOEPLITZ) {
-        const int *sh = &r.shape[3 * lvl];
-        const int nt = (2 * sh[0] - 1) * (2 * sh[1] - 1) * (2 * sh[2] - 1);
+        const int nt = tgeom(r, lvl, m.half_spectrum != 0).slen;
         S *out = ds + r.spec_off[node] * nrhs;
         const S *K0 = static_cast<const S *>(m.cpl);
         for (int q = 0; q < nq; ++q)
             for (int e = threadIdx.x; e < nt; e += blockDim.x) {
                 S acc = {0, 0};
+#pragma unroll 4
                 for (int p = p0; p < p1; ++p) {
                     const S *K = K0 + m.cpl_off[r.i2o_cpl[p]];
                     const S *in = as + t.spec_off[r.i2o_src[p]] * nrhs + (int64_t)q * nt;
@@ -444,112 +555,6 @@ __global__ void leaf_disaggregate_kernel(DMap m, DSide s, const int *__restrict_
     }
 }
 
-// ---------------------------------------------------------------------------------------------
-// D: near field. Forward: block per test leaf, thread per row, B read column by column.
-// Transposed: block per trial leaf, warp per output column of B, lanes along the column.
-// ---------------------------------------------------------------------------------------------
-template <class V>
-__global__ void near_forward_kernel(DNear n, DSide rs, DSide cs, int nrhs, const V *__restrict__ x,
-                                    int64_t ldx, V *__restrict__ y, int64_t ldy, V alpha, V beta,
-                                    bool beta_zero) {
-    __shared__ V xs[JT * RCH];
-    const int g = blockIdx.x;
-    const int row = n.row_leaf[g];
-    const int r0v = rs.value_ptr[row], nr = rs.value_ptr[row + 1] - r0v;
-    const int b0 = n.row_ptr[g], b1 = n.row_ptr[g + 1];
-    const V *D = static_cast<const V *>(n.data);
-    for (int r0 = 0; r0 < nrhs; r0 += RCH) {
-        const int rc = min(RCH, nrhs - r0);
-        for (int i0 = 0; i0 < nr; i0 += blockDim.x) {
-            const int i = i0 + threadIdx.x;
-            V acc[RCH];
-#pragma unroll
-            for (int q = 0; q < RCH; ++q) acc[q] = V{};
-            for (int bb = b0; bb < b1; ++bb) {
-                const int blk = n.row_blk[bb];
-                const int col = n.blk_col[blk];
-                const int c0v = cs.value_ptr[col], ncl = cs.value_ptr[col + 1] - c0v;
-                const V *B = D + n.blk_off[blk];
-                for (int j0 = 0; j0 < ncl; j0 += JT) {
-                    const int jt = min(JT, ncl - j0);
-                    __syncthreads();
-                    for (int e = threadIdx.x; e < JT * RCH; e += blockDim.x) {
-                        const int jj = e / RCH, q = e % RCH;
-                        xs[e] = (jj < jt && q < rc) ? x[(int64_t)(r0 + q) * ldx + cs.value[c0v + j0 + jj]] : V{};
-                    }
-                    __syncthreads();
-                    if (i < nr) {
-                        const V *bc = B + (int64_t)j0 * nr + i;
-#pragma unroll 8
-                        for (int jj = 0; jj < jt; ++jj) {
-                            const V bij = bc[(int64_t)jj * nr];
-#pragma unroll
-                            for (int q = 0; q < RCH; ++q) acc[q] = acc[q] + bij * xs[jj * RCH + q];
-                        }
-                    }
-                }
-            }
-            if (i < nr)
-                for (int q = 0; q < rc; ++q) {
-                    V *o = &y[(int64_t)(r0 + q) * ldy + rs.value[r0v + i]];
-                    const V v = alpha * acc[q];
-                    *o = beta_zero ? v : v + beta * *o;
-                }
-        }
-    }
-}
-
-template <class V>
-__global__ void near_transposed_kernel(DNear n, DSide rs, DSide cs, bool adj, int nrhs,
-                                       const V *__restrict__ x, int64_t ldx, V *__restrict__ y,
-                                       int64_t ldy, V alpha, V beta, bool beta_zero) {
-    extern __shared__ unsigned char smem_raw[];
-    V *acc = reinterpret_cast<V *>(smem_raw);  // [ncl][RCH]
-    const int g = blockIdx.x;
-    const int col = n.col_leaf[g];
-    const int c0v = cs.value_ptr[col], ncl = cs.value_ptr[col + 1] - c0v;
-    const int b0 = n.col_ptr[g], b1 = n.col_ptr[g + 1];
-    const V *D = static_cast<const V *>(n.data);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int r0 = 0; r0 < nrhs; r0 += RCH) {
-        const int rc = min(RCH, nrhs - r0);
-        for (int e = threadIdx.x; e < ncl * RCH; e += blockDim.x) acc[e] = V{};
-        __syncthreads();
-        for (int bb = b0; bb < b1; ++bb) {
-            const int blk = n.col_blk[bb];
-            const int row = n.blk_row[blk];
-            const int r0v = rs.value_ptr[row], nr = rs.value_ptr[row + 1] - r0v;
-            const V *B = D + n.blk_off[blk];
-            for (int j = warp; j < ncl; j += nw) {
-                const V *bc = B + (int64_t)j * nr;
-                V part[RCH];
-#pragma unroll
-                for (int q = 0; q < RCH; ++q) part[q] = V{};
-                for (int i = lane; i < nr; i += 32) {
-                    const V bij = cj(bc[i], adj);
-                    const int dof = rs.value[r0v + i];
-#pragma unroll
-                    for (int q = 0; q < RCH; ++q)
-                        if (q < rc) part[q] = part[q] + bij * x[(int64_t)(r0 + q) * ldx + dof];
-                }
-#pragma unroll
-                for (int q = 0; q < RCH; ++q) {
-                    const V s = warp_sum(part[q]);
-                    if (lane == 0) acc[j * RCH + q] = acc[j * RCH + q] + s;
-                }
-            }
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < ncl * rc; e += blockDim.x) {
-            const int j = e / rc, q = e % rc;
-            V *o = &y[(int64_t)(r0 + q) * ldy + cs.value[c0v + j]];
-            const V v = alpha * acc[j * RCH + q];
-            *o = beta_zero ? v : v + beta * *o;
-        }
-        __syncthreads();
-    }
-}
-
 template <class V>
 __global__ void zero_columns_kernel(int nrhs, int64_t n, V *y, int64_t ldy) {
     const int64_t total = n * nrhs;
@@ -614,10 +619,11 @@ cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DS
                                const int *nodes, int nnodes, bool conjt, const FarArgs &fa,
                                int maxcoef, int maxsep, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
-    const int bs = block_for(maxcoef);
+    const int bs = m.transfer_kind == H2B_TRANSFER_DENSE ? 256 : block_for(maxcoef);
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
-        const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? 0 : 3 * (size_t)maxsep * sizeof(T);
+        const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? (size_t)bs * sizeof(T)
+                                                                 : 3 * (size_t)maxsep * sizeof(T);
         err = allow_smem(transfer_up_kernel<T>, sm);
         if (err == cudaSuccess)
             transfer_up_kernel<T><<<nnodes, bs, sm, st>>>(m, s, nodes, conjt, fa.nrhs, static_cast<T *>(fa.am));
@@ -625,19 +631,29 @@ cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DS
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 
+namespace {
+int fft_groups(int maxt, size_t scalar) {
+    int g = 4;
+    while (g > 1 && (size_t)g * (maxt + 3 * FFT_NMAX) * scalar > 200 * 1024) --g;
+    return g;
+}
+}  // namespace
+
 cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DSide &s,
                                const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
                                int maxtsize, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
-    const int bs = block_for(maxtsize, 64, 512);
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
-        const size_t sm = (2 * (size_t)maxtsize + 128) * sizeof(S);
+        const int G = fft_groups(maxtsize, sizeof(S));
+        const size_t sm = (size_t)G * (maxtsize + 3 * FFT_NMAX) * sizeof(S);
+        const int ntrans = nnodes * m.ncomp * fa.nrhs;
         err = allow_smem(toeplitz_in_kernel<T>, sm);
         if (err == cudaSuccess)
-            toeplitz_in_kernel<T><<<nnodes, bs, sm, st>>>(m, s, nodes, inverse, fa.nrhs,
-                                                         static_cast<const T *>(fa.am), static_cast<S *>(fa.as));
+            toeplitz_in_kernel<T><<<(ntrans + G - 1) / G, G * FFT_T, sm, st>>>(
+                m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const T *>(fa.am),
+                static_cast<S *>(fa.as));
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
@@ -646,15 +662,17 @@ cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const D
                                 const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
                                 int maxtsize, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
-    const int bs = block_for(maxtsize, 64, 512);
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
-        const size_t sm = (2 * (size_t)maxtsize + 128) * sizeof(S);
+        const int G = fft_groups(maxtsize, sizeof(S));
+        const size_t sm = (size_t)G * (maxtsize + 3 * FFT_NMAX) * sizeof(S);
+        const int ntrans = nnodes * m.ncomp * fa.nrhs;
         err = allow_smem(toeplitz_out_kernel<T>, sm);
         if (err == cudaSuccess)
-            toeplitz_out_kernel<T><<<nnodes, bs, sm, st>>>(m, s, nodes, inverse, fa.nrhs,
-                                                          static_cast<const S *>(fa.ds), static_cast<T *>(fa.dm));
+            toeplitz_out_kernel<T><<<(ntrans + G - 1) / G, G * FFT_T, sm, st>>>(
+                m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const S *>(fa.ds),
+                static_cast<T *>(fa.dm));
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
@@ -663,8 +681,9 @@ cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &rec
                        const DSide &src, const int *nodes, int nnodes, const FarArgs &fa,
                        int maxcoef, int maxtsize, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
-    const int bs = m.coupling_kind == H2B_COUPLING_TOEPLITZ ? block_for(maxtsize, 64, 512)
-                                                            : block_for(maxcoef, 64, 256);
+    const int bs = m.coupling_kind == H2B_COUPLING_TOEPLITZ
+                       ? block_for(m.half_spectrum ? maxtsize / 2 + 64 : maxtsize, 64, 512)
+                       : block_for(maxcoef, 64, 256);
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
         i2o_kernel<T><<<nnodes, bs, 0, st>>>(m, recv, src, nodes, fa.mode, fa.nrhs,
@@ -709,44 +728,6 @@ cudaError_t launch_leaf_disaggregate(bool cplx, int precision, const DMap &m, co
             leaf_disaggregate_kernel<T, cdouble><<<nleaves, bs, 0, st>>>(
                 m, s, leaves, conjc, fa.nrhs, static_cast<const T *>(fa.dm), alpha, beta, bz,
                 static_cast<cdouble *>(y), ldy));
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &rows, const DSide &cols,
-                        int nrhs, const void *x, int64_t ldx, void *y, int64_t ldy, cdouble alpha,
-                        cdouble beta, int maxvals, cudaStream_t st) {
-    const bool adj = mode == H2B_ADJOINT;
-    if (mode == H2B_FORWARD) {
-        if (n.nrow_groups == 0) return cudaSuccess;
-        const int bs = block_for(maxvals, 64, 256);
-        if (!cplx)
-            near_forward_kernel<double><<<n.nrow_groups, bs, 0, st>>>(
-                n, rows, cols, nrhs, static_cast<const double *>(x), ldx, static_cast<double *>(y), ldy,
-                alpha.x, beta.x, beta.x == 0.0);
-        else
-            near_forward_kernel<cdouble><<<n.nrow_groups, bs, 0, st>>>(
-                n, rows, cols, nrhs, static_cast<const cdouble *>(x), ldx, static_cast<cdouble *>(y), ldy,
-                alpha, beta, beta.x == 0.0 && beta.y == 0.0);
-        return cudaGetLastError();
-    }
-    if (n.ncol_groups == 0) return cudaSuccess;
-    const int bs = 128;
-    cudaError_t err;
-    if (!cplx) {
-        const size_t sm = (size_t)maxvals * RCH * sizeof(double);
-        err = allow_smem(near_transposed_kernel<double>, sm);
-        if (err != cudaSuccess) return err;
-        near_transposed_kernel<double><<<n.ncol_groups, bs, sm, st>>>(
-            n, rows, cols, adj, nrhs, static_cast<const double *>(x), ldx, static_cast<double *>(y), ldy,
-            alpha.x, beta.x, beta.x == 0.0);
-    } else {
-        const size_t sm = (size_t)maxvals * RCH * sizeof(cdouble);
-        err = allow_smem(near_transposed_kernel<cdouble>, sm);
-        if (err != cudaSuccess) return err;
-        near_transposed_kernel<cdouble><<<n.ncol_groups, bs, sm, st>>>(
-            n, rows, cols, adj, nrhs, static_cast<const cdouble *>(x), ldx, static_cast<cdouble *>(y), ldy,
-            alpha, beta, beta.x == 0.0 && beta.y == 0.0);
     }
     return cudaGetLastError();
 }

@@ -1,0 +1,266 @@
+// Near field (nearmul!, src/nearinteractions/nearmul.jl:8-14) on sm_100a.
+//
+// Layout in HBM: every dense block of a (output leaf, input leaf) pair is stored column-major with
+// an even leading dimension for real fields, so that each lane of a warp streams two consecutive
+// rows with one 16-byte load. The blocks of one output leaf are split across the warps of one CTA;
+// every warp sweeps its blocks column by column with x broadcast from registers by shuffles, and
+// the warps' partial rows are summed in shared memory at the end. Transposed and adjoint products
+// run the same kernel on the transposed operator: N itself when N^T == N (checked once on the
+// device when the core is built), otherwise a transposed copy of the blocks built at upload.
+
+#include <algorithm>
+
+#include "h2b_internal.cuh"
+
+namespace h2b {
+
+namespace {
+
+constexpr int NEAR_WARPS = 8;
+
+template <class V> struct NearVec;
+template <> struct NearVec<double> {
+    static constexpr int RPL = 2;  // rows per lane per load
+};
+template <> struct NearVec<cdouble> {
+    static constexpr int RPL = 1;
+};
+
+__device__ __forceinline__ double shfl_idx(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ cdouble shfl_idx(cdouble v, int src) {
+    return {__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+
+// streaming (evict-first) loads of the near blocks: they are read once per product
+__device__ __forceinline__ void load_rows(const double *p, double (&v)[2]) {
+    const double2 t = __ldcs(reinterpret_cast<const double2 *>(p));
+    v[0] = t.x;
+    v[1] = t.y;
+}
+__device__ __forceinline__ void load_rows(const cdouble *p, cdouble (&v)[1]) {
+    const double2 t = __ldcs(reinterpret_cast<const double2 *>(p));
+    v[0] = {t.x, t.y};
+}
+
+__device__ __forceinline__ double fma_c(double a, double b, double c, bool) { return fma(a, b, c); }
+__device__ __forceinline__ cdouble fma_c(cdouble a, cdouble b, cdouble c, bool cjg) {
+    // c + op(a) * b, op = conj when cjg
+    const double ay = cjg ? -a.y : a.y;
+    return {fma(a.x, b.x, fma(-ay, b.y, c.x)), fma(a.x, b.y, fma(ay, b.x, c.y))};
+}
+
+__device__ __forceinline__ int near_ld(int nr, double *) { return nr + (nr & 1); }
+__device__ __forceinline__ int near_ld(int nr, cdouble *) { return nr; }
+
+// y[rows(g)] = alpha * op(N_g) x + beta * y[rows(g)] for right-hand sides [r0, r0 + R)
+template <class V, int R>
+__global__ void __launch_bounds__(NEAR_WARPS * 32)
+near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, const V *__restrict__ x,
+                 int64_t ldx, V *__restrict__ y, int64_t ldy, V alpha, V beta, bool beta_zero) {
+    constexpr int RPL = NearVec<V>::RPL;
+    constexpr int RPP = 32 * RPL;  // rows per pass
+    extern __shared__ unsigned char smem_raw[];
+    V *part = reinterpret_cast<V *>(smem_raw);  // [NEAR_WARPS][RPP][R]
+    const int g = blockIdx.x;
+    const int leaf = op.grp_leaf[g];
+    const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
+    const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const V *D = static_cast<const V *>(op.data);
+    const int ld = near_ld(nr, (V *)nullptr);
+    for (int p0 = 0; p0 < nr; p0 += RPP) {
+        const int i0 = p0 + RPL * lane;  // first row of this lane
+        V acc[RPL][R];
+#pragma unroll
+        for (int k = 0; k < RPL; ++k)
+#pragma unroll
+            for (int q = 0; q < R; ++q) acc[k][q] = V{};
+        for (int bb = b0 + warp; bb < b1; bb += NEAR_WARPS) {
+            const int blk = op.grp_blk[bb];
+            const int inl = op.blk_in[blk];
+            const int c0 = ins.value_ptr[inl], nc = ins.value_ptr[inl + 1] - c0;
+            const V *B = D + op.blk_off[blk] + i0;
+            for (int j0 = 0; j0 < nc; j0 += 32) {
+                V xr[R];
+                const int jl = j0 + lane;
+                if (jl < nc) {
+                    const int dof = ins.value[c0 + jl];
+#pragma unroll
+                    for (int q = 0; q < R; ++q) xr[q] = q < rc ? x[(int64_t)(r0 + q) * ldx + dof] : V{};
+                } else {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) xr[q] = V{};
+                }
+                const int jn = min(32, nc - j0);
+                const bool live = i0 < nr;  // lanes past the last row load nothing but still shuffle
+#pragma unroll 4
+                for (int jj = 0; jj < jn; ++jj) {
+                    V bv[RPL];
+                    if (live) {
+                        load_rows(B + (int64_t)(j0 + jj) * ld, bv);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < RPL; ++k) bv[k] = V{};
+                    }
+#pragma unroll
+                    for (int q = 0; q < R; ++q) {
+                        const V xv = shfl_idx(xr[q], jj);
+#pragma unroll
+                        for (int k = 0; k < RPL; ++k) acc[k][q] = fma_c(bv[k], xv, acc[k][q], cjg);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RPL; ++k)
+#pragma unroll
+            for (int q = 0; q < R; ++q) part[(warp * RPP + RPL * lane + k) * R + q] = acc[k][q];
+        __syncthreads();
+        const int rows = min(RPP, nr - p0);
+        for (int e = threadIdx.x; e < rows * rc; e += blockDim.x) {
+            const int i = e / rc, q = e % rc;
+            V s = V{};
+#pragma unroll
+            for (int w = 0; w < NEAR_WARPS; ++w) s = s + part[(w * RPP + i) * R + q];
+            V *o = &y[(int64_t)(r0 + q) * ldy + outs.value[o0 + p0 + i]];
+            const V v = alpha * s;
+            *o = beta_zero ? v : v + beta * *o;
+        }
+        __syncthreads();
+    }
+}
+
+// Build-time helpers --------------------------------------------------------------------------
+// Copy block b (nr x nc, column-major, leading dimension nr) into the padded layout; with
+// `transpose`, write its transpose (nc x nr) instead.
+template <class V>
+__global__ void near_repack_kernel(const V *__restrict__ src, const int64_t *__restrict__ src_off,
+                                   const int *__restrict__ blk_row, const int *__restrict__ blk_col,
+                                   DSide rows, DSide cols, V *__restrict__ dst,
+                                   const int64_t *__restrict__ dst_off, bool transpose) {
+    const int b = blockIdx.x;
+    const int r = blk_row[b], c = blk_col[b];
+    const int nr = rows.value_ptr[r + 1] - rows.value_ptr[r];
+    const int nc = cols.value_ptr[c + 1] - cols.value_ptr[c];
+    const V *s = src + src_off[b];
+    V *d = dst + dst_off[b];
+    if (!transpose) {
+        const int ld = near_ld(nr, (V *)nullptr);
+        for (int64_t e = threadIdx.x; e < (int64_t)ld * nc; e += blockDim.x) {
+            const int i = (int)(e % ld), j = (int)(e / ld);
+            d[e] = i < nr ? s[i + (int64_t)j * nr] : V{};
+        }
+    } else {
+        const int ld = near_ld(nc, (V *)nullptr);
+        for (int64_t e = threadIdx.x; e < (int64_t)ld * nr; e += blockDim.x) {
+            const int j = (int)(e % ld), i = (int)(e / ld);
+            d[e] = j < nc ? s[i + (int64_t)j * nr] : V{};
+        }
+    }
+}
+
+__device__ __forceinline__ bool same(double a, double b) { return a == b; }
+__device__ __forceinline__ bool same(cdouble a, cdouble b) { return a.x == b.x && a.y == b.y; }
+
+// flag stays 1 only if every block equals the transpose of its mirror block
+template <class V>
+__global__ void near_symcheck_kernel(const V *__restrict__ src, const int64_t *__restrict__ off,
+                                     const int *__restrict__ mirror, const int *__restrict__ blk_row,
+                                     DSide rows, int *__restrict__ flag) {
+    const int b = blockIdx.x;
+    const int m = mirror[b];
+    const int r = blk_row[b];
+    const int nr = rows.value_ptr[r + 1] - rows.value_ptr[r];
+    const int nc = rows.value_ptr[blk_row[m] + 1] - rows.value_ptr[blk_row[m]];
+    const V *s = src + off[b];
+    const V *t = src + off[m];
+    bool ok = true;
+    for (int64_t e = threadIdx.x; e < (int64_t)nr * nc; e += blockDim.x) {
+        const int i = (int)(e % nr), j = (int)(e / nr);
+        ok &= same(s[e], t[j + (int64_t)i * nc]);
+    }
+    if (!__syncthreads_and(ok) && threadIdx.x == 0) *flag = 0;
+}
+
+template <class V, int R>
+cudaError_t launch_rows_t(const NearOp &op, const DSide &outs, const DSide &ins, bool cjg, int r0,
+                          int rc, const V *x, int64_t ldx, V *y, int64_t ldy, V alpha, V beta,
+                          bool bz, cudaStream_t st) {
+    constexpr int RPP = 32 * NearVec<V>::RPL;
+    const size_t sm = (size_t)NEAR_WARPS * RPP * R * sizeof(V);
+    cudaError_t e = cudaSuccess;
+    if (sm > 48 * 1024)
+        e = cudaFuncSetAttribute(near_rows_kernel<V, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    near_rows_kernel<V, R><<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, cjg, r0, rc, x, ldx, y,
+                                                                     ldy, alpha, beta, bz);
+    return cudaGetLastError();
+}
+
+template <class V>
+cudaError_t near_apply_t(const NearOp &op, const DSide &outs, const DSide &ins, bool cjg, int nrhs,
+                         const V *x, int64_t ldx, V *y, int64_t ldy, V alpha, V beta, bool bz,
+                         cudaStream_t st) {
+    if (op.ngroups == 0) return cudaSuccess;
+    for (int r0 = 0; r0 < nrhs; r0 += 16) {
+        const int rc = std::min(16, nrhs - r0);
+        cudaError_t e;
+        if (rc == 1) e = launch_rows_t<V, 1>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        else if (rc == 2) e = launch_rows_t<V, 2>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        else if (rc <= 4) e = launch_rows_t<V, 4>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        else if (rc <= 8) e = launch_rows_t<V, 8>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        else e = launch_rows_t<V, 16>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+int64_t near_padded_ld(bool cplx, int n) { return cplx ? n : n + (n & 1); }
+
+cudaError_t launch_near_repack(bool cplx, const void *src, const int64_t *src_off, const int *blk_row,
+                               const int *blk_col, const DSide &rows, const DSide &cols, void *dst,
+                               const int64_t *dst_off, int nblocks, bool transpose, cudaStream_t st) {
+    if (nblocks == 0) return cudaSuccess;
+    if (cplx)
+        near_repack_kernel<cdouble><<<nblocks, 256, 0, st>>>(static_cast<const cdouble *>(src), src_off, blk_row,
+                                                             blk_col, rows, cols, static_cast<cdouble *>(dst),
+                                                             dst_off, transpose);
+    else
+        near_repack_kernel<double><<<nblocks, 256, 0, st>>>(static_cast<const double *>(src), src_off, blk_row,
+                                                            blk_col, rows, cols, static_cast<double *>(dst),
+                                                            dst_off, transpose);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_near_symcheck(bool cplx, const void *src, const int64_t *off, const int *mirror,
+                                 const int *blk_row, const DSide &rows, int nblocks, int *flag,
+                                 cudaStream_t st) {
+    if (nblocks == 0) return cudaSuccess;
+    if (cplx)
+        near_symcheck_kernel<cdouble><<<nblocks, 256, 0, st>>>(static_cast<const cdouble *>(src), off, mirror,
+                                                               blk_row, rows, flag);
+    else
+        near_symcheck_kernel<double><<<nblocks, 256, 0, st>>>(static_cast<const double *>(src), off, mirror,
+                                                              blk_row, rows, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &test, const DSide &trial,
+                        int nrhs, const void *x, int64_t ldx, void *y, int64_t ldy, cdouble alpha,
+                        cdouble beta, cudaStream_t st) {
+    const bool fwd_op = mode == H2B_FORWARD || n.symmetric;
+    const NearOp &op = fwd_op ? n.fwd : n.tr;
+    const DSide &outs = fwd_op ? test : trial;
+    const DSide &ins = fwd_op ? trial : test;
+    const bool cjg = mode == H2B_ADJOINT && cplx;
+    if (cplx)
+        return near_apply_t<cdouble>(op, outs, ins, cjg, nrhs, static_cast<const cdouble *>(x), ldx,
+                                     static_cast<cdouble *>(y), ldy, alpha, beta,
+                                     beta.x == 0.0 && beta.y == 0.0, st);
+    return near_apply_t<double>(op, outs, ins, false, nrhs, static_cast<const double *>(x), ldx,
+                                static_cast<double *>(y), ldy, alpha.x, beta.x, beta.x == 0.0, st);
+}
+
+}  // namespace h2b
