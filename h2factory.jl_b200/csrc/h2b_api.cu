@@ -10,6 +10,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
 #include <vector>
@@ -64,6 +65,7 @@ struct SideHost {
     std::vector<int> level, shape;
     int maxcoef = 1, maxtsize = 1, maxvals = 1;
     int maxsep = 1;  // bound on separable-contraction intermediates between adjacent levels
+    int maxaxis = 1; // longest padded Toeplitz axis (2s - 1)
     int64_t mom_total = 0, spec_total = 0;  // per unit right-hand side
     int *d_agg_leaves = nullptr;
     int n_agg_leaves = 0;
@@ -77,6 +79,9 @@ struct SideHost {
     int *d_init_leaves = nullptr;
     int n_init_leaves = 0;
     int64_t npairs = 0;
+    std::vector<int64_t> mom_off_host;  // moment offsets per unit rhs (host copy)
+    std::vector<int64_t> spec_off_host; // spectrum offsets per unit rhs (host copy)
+    int maxhalf = 1;                    // longest stored (half) spectrum
     DSide d{};
 };
 
@@ -417,6 +422,7 @@ h2b_status build_side(h2b_core *c, const h2b_map_desc &d, const h2b_side_desc &s
     for (int l = 1; l <= s.nlevels; ++l) {
         h.maxcoef = std::max<int>(h.maxcoef, (int)ncoef_host(s, l));
         h.maxtsize = std::max<int>(h.maxtsize, (int)tsize_host(s, l));
+        for (int k = 0; k < 3; ++k) h.maxaxis = std::max(h.maxaxis, 2 * s.shape[3 * l + k] - 1);
         if (l > 1) {
             int b = 1;
             for (int k = 0; k < 3; ++k) b *= std::max(s.shape[3 * l + k], s.shape[3 * (l - 1) + k]);
@@ -521,6 +527,10 @@ h2b_status build_side(h2b_core *c, const h2b_map_desc &d, const h2b_side_desc &s
     if (st) return st;
     CUDA_TRY(c->upload(&h.d_received, received.data(), received.size()));
     (void)other;
+    h.mom_off_host = mo;
+    h.spec_off_host = so;
+    for (int l = 1; l <= s.nlevels; ++l)
+        h.maxhalf = std::max<int>(h.maxhalf, (int)spec_len(s, l, c->dmap.half_spectrum != 0));
     return H2B_OK;
 }
 
@@ -740,6 +750,21 @@ h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
     int64_t *q;
     CUDA_TRY(c->upload(&q, off.data(), off.size()));
     M.cpl_off = q;
+    // per-pair operand offsets for the I2O kernel (both sides; sources live on the other side)
+    for (int side = 0; side < 2; ++side) {
+        const h2b_side_desc &sd = side == 0 ? d.test : d.trial;
+        SideHost &h = side == 0 ? c->test : c->trial;
+        const SideHost &o = side == 0 ? c->trial : c->test;
+        const int np = sd.i2o_ptr[sd.nnodes];
+        std::vector<int64_t> psrc(std::max(np, 1)), pcpl(std::max(np, 1));
+        for (int p = 0; p < np; ++p) {
+            const int src = sd.i2o_src[p];
+            psrc[p] = toep ? o.spec_off_host[src] : o.mom_off_host[src];
+            pcpl[p] = off[sd.i2o_coupling[p]];
+        }
+        CUDA_TRY(c->upload(&q, psrc.data(), psrc.size())); h.d.pair_src = q;
+        CUDA_TRY(c->upload(&q, pcpl.data(), pcpl.size())); h.d.pair_cpl = q;
+    }
     return build_near(c, d);
 }
 
@@ -877,6 +902,15 @@ struct BusyGuard {
     }
 };
 
+// I2O of all receiving nodes of side D from the moments / spectra of side A.
+h2b_status run_i2o(h2b_core *c, const SideHost &D, const SideHost &A, const FarArgs &fa, cudaStream_t st) {
+    const int maxcoef = std::max(A.maxcoef, D.maxcoef);
+    const int maxt = std::max(A.maxtsize, D.maxtsize);
+    CUDA_TRY(launch_i2o(c->field == H2B_COMPLEX, c->precision, c->dmap, D.d, A.d, D.d_recv, D.n_recv, fa,
+                        maxcoef, maxt, D.maxhalf, st));
+    return H2B_OK;
+}
+
 h2b_status far_passes(h2b_workspace *ws, int mode, int nrhs, const void *x, int64_t ldx, void *y,
                       int64_t ldy, cdouble alpha_eff, cdouble beta, cudaStream_t st,
                       cudaEvent_t wait_before_scatter) {
@@ -897,11 +931,14 @@ h2b_status far_passes(h2b_workspace *ws, int mode, int nrhs, const void *x, int6
                                     A.maxcoef, A.maxsep, st));
     if (toep)
         CUDA_TRY(launch_toeplitz_in(cplx, pr, c->dmap, A.d, A.d_store, A.n_store, mode == H2B_TRANSPOSE,
-                                    fa, A.maxtsize, st));
-    CUDA_TRY(launch_i2o(cplx, pr, c->dmap, D.d, A.d, D.d_recv, D.n_recv, fa, maxcoef, maxt, st));
+                                    fa, A.maxtsize, A.maxaxis, st));
+    {
+        const h2b_status si = run_i2o(c, D, A, fa, st);
+        if (si) return si;
+    }
     if (toep)
         CUDA_TRY(launch_toeplitz_out(cplx, pr, c->dmap, D.d, D.d_recv, D.n_recv, mode != H2B_TRANSPOSE,
-                                     fa, D.maxtsize, st));
+                                     fa, D.maxtsize, D.maxaxis, st));
     for (const Stage &sg : D.dis_down)
         CUDA_TRY(launch_transfer_down(cplx, pr, c->dmap, D.d, sg.d_nodes, sg.n, D.d_received, fa,
                                       D.maxcoef, D.maxsep, st));
@@ -1075,11 +1112,14 @@ h2b_status far_passes_scratch(h2b_core *c, const FarArgs &fa, const void *x, int
                                     A.maxcoef, A.maxsep, st));
     if (toep)
         CUDA_TRY(launch_toeplitz_in(cplx, pr, c->dmap, A.d, A.d_store, A.n_store, mode == H2B_TRANSPOSE,
-                                    fa, A.maxtsize, st));
-    CUDA_TRY(launch_i2o(cplx, pr, c->dmap, D.d, A.d, D.d_recv, D.n_recv, fa, maxcoef, maxt, st));
+                                    fa, A.maxtsize, A.maxaxis, st));
+    {
+        const h2b_status si = run_i2o(c, D, A, fa, st);
+        if (si) return si;
+    }
     if (toep)
         CUDA_TRY(launch_toeplitz_out(cplx, pr, c->dmap, D.d, D.d_recv, D.n_recv, mode != H2B_TRANSPOSE,
-                                     fa, D.maxtsize, st));
+                                     fa, D.maxtsize, D.maxaxis, st));
     for (const Stage &sg : D.dis_down)
         CUDA_TRY(launch_transfer_down(cplx, pr, c->dmap, D.d, sg.d_nodes, sg.n, D.d_received, fa,
                                       D.maxcoef, D.maxsep, st));

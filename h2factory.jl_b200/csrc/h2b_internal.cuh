@@ -75,7 +75,9 @@ struct DSide {
     const int64_t *tr_off;   // [(nlevels+1)*nsectors] transfer offsets (elements of T)
     const void *tr;          // T
     const int *i2o_ptr, *i2o_src;
-    const int64_t *i2o_cpl;  // coupling index of each pair
+    const int64_t *i2o_cpl;   // coupling index of each pair
+    const int64_t *pair_src;  // per pair: the source's moment / spectrum offset per unit rhs
+    const int64_t *pair_cpl;  // per pair: the coupling's element offset in the coupling array
 };
 
 struct DMap {
@@ -126,13 +128,13 @@ cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DS
                                int maxcoef, int maxsep, cudaStream_t st);
 cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DSide &s,
                                const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
-                               int maxtsize, cudaStream_t st);
+                               int maxtsize, int maxaxis, cudaStream_t st);
 cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &recv,
                        const DSide &src, const int *nodes, int nnodes, const FarArgs &fa,
-                       int maxcoef, int maxtsize, cudaStream_t st);
+                       int maxcoef, int maxtsize, int maxhalf, cudaStream_t st);
 cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const DSide &s,
                                 const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
-                                int maxtsize, cudaStream_t st);
+                                int maxtsize, int maxaxis, cudaStream_t st);
 cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const DSide &s,
                                  const int *nodes, int nnodes, const uint8_t *received,
                                  const FarArgs &fa, int maxcoef, int maxsep, cudaStream_t st);

@@ -255,31 +255,24 @@ __device__ __forceinline__ void dft_line(Cx<R> *a, int base, int stride, const C
     }
 }
 
-template <class R>
+// Padded extents are 2s - 1, hence odd; NMAX bounds the longest line (register footprint).
+template <class R, int NMAX>
 __device__ __forceinline__ void dft_line_n(int n, Cx<R> *a, int base, int stride, const Cx<R> *tw, R scale) {
     switch (n) {
-    case 2: dft_line<R, 2>(a, base, stride, tw, scale); break;
     case 3: dft_line<R, 3>(a, base, stride, tw, scale); break;
-    case 4: dft_line<R, 4>(a, base, stride, tw, scale); break;
     case 5: dft_line<R, 5>(a, base, stride, tw, scale); break;
-    case 6: dft_line<R, 6>(a, base, stride, tw, scale); break;
     case 7: dft_line<R, 7>(a, base, stride, tw, scale); break;
-    case 8: dft_line<R, 8>(a, base, stride, tw, scale); break;
-    case 9: dft_line<R, 9>(a, base, stride, tw, scale); break;
-    case 10: dft_line<R, 10>(a, base, stride, tw, scale); break;
-    case 11: dft_line<R, 11>(a, base, stride, tw, scale); break;
-    case 12: dft_line<R, 12>(a, base, stride, tw, scale); break;
-    case 13: dft_line<R, 13>(a, base, stride, tw, scale); break;
-    case 14: dft_line<R, 14>(a, base, stride, tw, scale); break;
-    case 15: dft_line<R, 15>(a, base, stride, tw, scale); break;
-    case 16: dft_line<R, 16>(a, base, stride, tw, scale); break;
+    case 9: if (NMAX >= 9) dft_line<R, (NMAX >= 9 ? 9 : 3)>(a, base, stride, tw, scale); break;
+    case 11: if (NMAX >= 11) dft_line<R, (NMAX >= 11 ? 11 : 3)>(a, base, stride, tw, scale); break;
+    case 13: if (NMAX >= 13) dft_line<R, (NMAX >= 13 ? 13 : 3)>(a, base, stride, tw, scale); break;
+    case 15: if (NMAX >= 15) dft_line<R, (NMAX >= 15 ? 15 : 3)>(a, base, stride, tw, scale); break;
     default: break;
     }
 }
 
 // In-place multidimensional DFT of one transform held by FFT_T threads (tl = thread in group).
 // Every thread of the CTA calls this the same number of times (3 barriers), busy or not.
-template <class R>
+template <class R, int NMAX>
 __device__ void dft_group(Cx<R> *a, const TGeom &g, bool inverse, Cx<R> *tw, int tl, bool busy) {
     // twiddles of the three axes: tw[16 * ax + k] = e^{-+2 pi i k / n}
     if (busy)
@@ -310,7 +303,7 @@ __device__ void dft_group(Cx<R> *a, const TGeom &g, bool inverse, Cx<R> *tw, int
                     base = l;
                     stride = g.ts[0] * g.ts[1];
                 }
-                dft_line_n(n, a, base, stride, tw + FFT_NMAX * ax, scale);
+                dft_line_n<R, NMAX>(n, a, base, stride, tw + FFT_NMAX * ax, scale);
             }
         }
         __syncthreads();
@@ -318,8 +311,8 @@ __device__ void dft_group(Cx<R> *a, const TGeom &g, bool inverse, Cx<R> *tw, int
 }
 
 // A3: spectrum(node) = F(pad(moment(node)))   (F = fft, or ifft for transpose maps)
-template <class T>
-__global__ void toeplitz_in_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
+template <class T, int NMAX>
+__global__ void __launch_bounds__(256) toeplitz_in_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
                                    int nrhs, int maxt, const T *__restrict__ am,
                                    typename ScalarTraits<T>::Complex *__restrict__ as) {
     using S = typename ScalarTraits<T>::Complex;
@@ -344,7 +337,7 @@ __global__ void toeplitz_in_kernel(DMap m, DSide s, const int *__restrict__ node
             a[e] = v;
         }
     }
-    dft_group<R>(a, g, inverse, tw, tl, busy);
+    dft_group<R, NMAX>(a, g, inverse, tw, tl, busy);
     if (busy) {
         S *spec = as + s.spec_off[node] * nrhs + (int64_t)q * g.slen;
         for (int e = tl; e < g.slen; e += FFT_T) {
@@ -355,8 +348,8 @@ __global__ void toeplitz_in_kernel(DMap m, DSide s, const int *__restrict__ node
 }
 
 // B3: moment(node) = corner(F^-1(spectrum(node)))   (overwrite)
-template <class T>
-__global__ void toeplitz_out_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
+template <class T, int NMAX>
+__global__ void __launch_bounds__(256) toeplitz_out_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
                                     int nrhs, int maxt,
                                     const typename ScalarTraits<T>::Complex *__restrict__ ds,
                                     T *__restrict__ dm) {
@@ -385,7 +378,7 @@ __global__ void toeplitz_out_kernel(DMap m, DSide s, const int *__restrict__ nod
             }
         }
     }
-    dft_group<R>(a, g, inverse, tw, tl, busy);
+    dft_group<R, NMAX>(a, g, inverse, tw, tl, busy);
     if (busy) {
         T *mom = dm + s.mom_off[node] * nrhs + (int64_t)q * g.nc;
         for (int e = tl; e < g.nc; e += FFT_T) {
@@ -413,6 +406,8 @@ __global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nod
     const int nc = ncoef_of(r, lvl);
     const int nq = m.ncomp * nrhs;
     const bool adj = (mode == H2B_ADJOINT);
+    // r.pair_src[p]: the source's moment (or spectrum) offset per unit rhs; r.pair_cpl[p]: the
+    // coupling's element offset -- one load each per pair, no chained index lookups
     if (m.coupling_kind == H2B_COUPLING_TOEPLITZ) {
         const int nt = tgeom(r, lvl, m.half_spectrum != 0).slen;
         S *out = ds + r.spec_off[node] * nrhs;
@@ -420,12 +415,19 @@ __global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nod
         for (int q = 0; q < nq; ++q)
             for (int e = threadIdx.x; e < nt; e += blockDim.x) {
                 S acc = {0, 0};
-#pragma unroll 4
-                for (int p = p0; p < p1; ++p) {
-                    const S *K = K0 + m.cpl_off[r.i2o_cpl[p]];
-                    const S *in = as + t.spec_off[r.i2o_src[p]] * nrhs + (int64_t)q * nt;
-                    acc = acc + cj(K[e], adj) * in[e];
+                int p = p0;
+                for (; p + 4 <= p1; p += 4) {
+                    S kv[4], iv[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        kv[u] = K0[r.pair_cpl[p + u] + e];
+                        iv[u] = as[r.pair_src[p + u] * nrhs + (int64_t)q * nt + e];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc = acc + cj(kv[u], adj) * iv[u];
                 }
+                for (; p < p1; ++p)
+                    acc = acc + cj(K0[r.pair_cpl[p] + e], adj) * as[r.pair_src[p] * nrhs + (int64_t)q * nt + e];
                 out[(int64_t)q * nt + e] = acc;
             }
         return;
@@ -437,10 +439,8 @@ __global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nod
             for (int a = threadIdx.x; a < nc; a += blockDim.x) {
                 T acc = sc_zero<T>();
                 for (int p = p0; p < p1; ++p) {
-                    const int src = r.i2o_src[p];
-                    const int snc = ncoef_of(t, t.level[src]);
-                    const T *D = B0 + m.cpl_off[r.i2o_cpl[p]];
-                    acc = acc + cj(D[a], adj) * am[t.mom_off[src] * nrhs + (int64_t)q * snc + a];
+                    const T *D = B0 + r.pair_cpl[p];
+                    acc = acc + cj(D[a], adj) * am[r.pair_src[p] * nrhs + (int64_t)q * nc + a];
                 }
                 out[(int64_t)q * nc + a] = acc;
             }
@@ -452,10 +452,9 @@ __global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nod
             for (int a = threadIdx.x; a < nc; a += blockDim.x) {
                 T acc = sc_zero<T>();
                 for (int p = p0; p < p1; ++p) {
-                    const int src = r.i2o_src[p];
-                    const int snc = ncoef_of(t, t.level[src]);
-                    const T *B = B0 + m.cpl_off[r.i2o_cpl[p]];
-                    const T *in = am + t.mom_off[src] * nrhs + (int64_t)q * snc;
+                    const int snc = ncoef_of(t, t.level[r.i2o_src[p]]);
+                    const T *B = B0 + r.pair_cpl[p];
+                    const T *in = am + r.pair_src[p] * nrhs + (int64_t)q * snc;
                     for (int b = 0; b < snc; ++b) acc = acc + B[a + (int64_t)b * nc] * in[b];
                 }
                 out[(int64_t)q * nc + a] = acc;
@@ -468,10 +467,9 @@ __global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nod
         for (int a = warp; a < nc; a += nw) {
             T acc = sc_zero<T>();
             for (int p = p0; p < p1; ++p) {
-                const int src = r.i2o_src[p];
-                const int snc = ncoef_of(t, t.level[src]);
-                const T *B = B0 + m.cpl_off[r.i2o_cpl[p]] + (int64_t)a * snc;
-                const T *in = am + t.mom_off[src] * nrhs + (int64_t)q * snc;
+                const int snc = ncoef_of(t, t.level[r.i2o_src[p]]);
+                const T *B = B0 + r.pair_cpl[p] + (int64_t)a * snc;
+                const T *in = am + r.pair_src[p] * nrhs + (int64_t)q * snc;
                 for (int b = lane; b < snc; b += 32) acc = acc + cj(B[b], adj) * in[b];
             }
             acc = warp_sum(acc);
@@ -641,7 +639,7 @@ int fft_groups(int maxt, size_t scalar) {
 
 cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DSide &s,
                                const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
-                               int maxtsize, cudaStream_t st) {
+                               int maxtsize, int maxaxis, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
@@ -649,18 +647,24 @@ cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DS
         const int G = fft_groups(maxtsize, sizeof(S));
         const size_t sm = (size_t)G * (maxtsize + 3 * FFT_NMAX) * sizeof(S);
         const int ntrans = nnodes * m.ncomp * fa.nrhs;
-        err = allow_smem(toeplitz_in_kernel<T>, sm);
-        if (err == cudaSuccess)
-            toeplitz_in_kernel<T><<<(ntrans + G - 1) / G, G * FFT_T, sm, st>>>(
-                m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const T *>(fa.am),
-                static_cast<S *>(fa.as));
+        auto launch = [&](auto kern) {
+            cudaError_t e2 = allow_smem(kern, sm);
+            if (e2 == cudaSuccess)
+                e2 = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared);
+            if (e2 == cudaSuccess)
+                kern<<<(ntrans + G - 1) / G, G * FFT_T, sm, st>>>(
+                    m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const T *>(fa.am), static_cast<S *>(fa.as));
+            return e2;
+        };
+        err = maxaxis <= 7 ? launch(toeplitz_in_kernel<T, 7>) : launch(toeplitz_in_kernel<T, 15>);
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 
 cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const DSide &s,
                                 const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
-                                int maxtsize, cudaStream_t st) {
+                                int maxtsize, int maxaxis, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
@@ -668,21 +672,28 @@ cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const D
         const int G = fft_groups(maxtsize, sizeof(S));
         const size_t sm = (size_t)G * (maxtsize + 3 * FFT_NMAX) * sizeof(S);
         const int ntrans = nnodes * m.ncomp * fa.nrhs;
-        err = allow_smem(toeplitz_out_kernel<T>, sm);
-        if (err == cudaSuccess)
-            toeplitz_out_kernel<T><<<(ntrans + G - 1) / G, G * FFT_T, sm, st>>>(
-                m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const S *>(fa.ds),
-                static_cast<T *>(fa.dm));
+        auto launch = [&](auto kern) {
+            cudaError_t e2 = allow_smem(kern, sm);
+            if (e2 == cudaSuccess)
+                e2 = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared);
+            if (e2 == cudaSuccess)
+                kern<<<(ntrans + G - 1) / G, G * FFT_T, sm, st>>>(
+                    m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const S *>(fa.ds), static_cast<T *>(fa.dm));
+            return e2;
+        };
+        err = maxaxis <= 7 ? launch(toeplitz_out_kernel<T, 7>) : launch(toeplitz_out_kernel<T, 15>);
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 
 cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &recv,
                        const DSide &src, const int *nodes, int nnodes, const FarArgs &fa,
-                       int maxcoef, int maxtsize, cudaStream_t st) {
+                       int maxcoef, int maxtsize, int maxhalf, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
+    // Toeplitz: one thread per stored frequency (half spectra hold (n1/2 + 1) * n2 * n3 of them)
     const int bs = m.coupling_kind == H2B_COUPLING_TOEPLITZ
-                       ? block_for(m.half_spectrum ? maxtsize / 2 + 64 : maxtsize, 64, 512)
+                       ? block_for(m.half_spectrum ? maxhalf : maxtsize, 32, 512)
                        : block_for(maxcoef, 64, 256);
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;

@@ -75,12 +75,15 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
         for (int k = 0; k < RPL; ++k)
 #pragma unroll
             for (int q = 0; q < R; ++q) acc[k][q] = V{};
-        for (int bb = b0 + warp; bb < b1; bb += NEAR_WARPS) {
+        // work units are (block, 32-column chunk) pairs, dealt round-robin to the warps
+        int unit = 0;
+        for (int bb = b0; bb < b1; ++bb) {
             const int blk = op.grp_blk[bb];
             const int inl = op.blk_in[blk];
             const int c0 = ins.value_ptr[inl], nc = ins.value_ptr[inl + 1] - c0;
             const V *B = D + op.blk_off[blk] + i0;
-            for (int j0 = 0; j0 < nc; j0 += 32) {
+            for (int j0 = 0; j0 < nc; j0 += 32, ++unit) {
+                if (unit % NEAR_WARPS != warp) continue;
                 V xr[R];
                 const int jl = j0 + lane;
                 if (jl < nc) {
@@ -93,11 +96,32 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
                 }
                 const int jn = min(32, nc - j0);
                 const bool live = i0 < nr;  // lanes past the last row load nothing but still shuffle
-#pragma unroll 4
-                for (int jj = 0; jj < jn; ++jj) {
+                const V *Bj = B + (int64_t)j0 * ld;
+                int jj = 0;
+                for (; jj + 8 <= jn; jj += 8) {
+                    V bv[8][RPL];  // eight columns in flight before any use
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        if (live) {
+                            load_rows(Bj + (int64_t)(jj + u) * ld, bv[u]);
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < RPL; ++k) bv[u][k] = V{};
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+#pragma unroll
+                        for (int q = 0; q < R; ++q) {
+                            const V xv = shfl_idx(xr[q], jj + u);
+#pragma unroll
+                            for (int k = 0; k < RPL; ++k) acc[k][q] = fma_c(bv[u][k], xv, acc[k][q], cjg);
+                        }
+                }
+                for (; jj < jn; ++jj) {
                     V bv[RPL];
                     if (live) {
-                        load_rows(B + (int64_t)(j0 + jj) * ld, bv);
+                        load_rows(Bj + (int64_t)jj * ld, bv);
                     } else {
 #pragma unroll
                         for (int k = 0; k < RPL; ++k) bv[k] = V{};
