@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -79,6 +80,8 @@ struct SideHost {
     int *d_init_leaves = nullptr;
     int n_init_leaves = 0;
     int64_t npairs = 0;
+    SibGroups sib;                      // Toeplitz I2O by sibling groups (ngroups = 0: per node)
+    int maxslen = 1;
     std::vector<int64_t> mom_off_host;  // moment offsets per unit rhs (host copy)
     std::vector<int64_t> spec_off_host; // spectrum offsets per unit rhs (host copy)
     int maxhalf = 1;                    // longest stored (half) spectrum
@@ -409,6 +412,64 @@ h2b_status upload_far_scalars(h2b_core *c, const double *src, int64_t count, con
 
 h2b_status upload_list(h2b_core *c, const std::vector<int> &v, int **dst) {
     CUDA_TRY(c->upload(dst, v.data(), v.size()));
+    return H2B_OK;
+}
+
+// Sibling groups of the receiving nodes of side `s` for the Toeplitz I2O: the receiving children
+// of each parent, with the union of their sources and, per (source, child slot), the coupling's
+// element offset. Left empty (per-node kernel) when a receiver has no parent or a child slot
+// beyond 8, or lists one source twice.
+h2b_status build_sibling_groups(h2b_core *c, const h2b_side_desc &s, SideHost &h,
+                                const std::vector<int64_t> &other_spec_off,
+                                const std::vector<int64_t> &cpl_elem_off) {
+    std::vector<int> recv;
+    for (int n = 0; n < s.nnodes; ++n)
+        if (s.i2o_ptr[n + 1] > s.i2o_ptr[n]) recv.push_back(n);
+    std::map<int, int> gidx;
+    std::vector<int> grecv;
+    for (int n : recv) {
+        if (n == s.root || s.sector[n] >= 8) return H2B_OK;
+        auto it = gidx.find(s.parent[n]);
+        if (it == gidx.end()) {
+            it = gidx.emplace(s.parent[n], (int)gidx.size()).first;
+            grecv.insert(grecv.end(), 8, -1);
+        }
+        grecv[it->second * 8 + s.sector[n]] = n;
+    }
+    const int ng = (int)gidx.size();
+    std::vector<int> gptr{0}, gslen(ng), gkof;
+    std::vector<int64_t> gsrc;
+    for (int gi = 0; gi < ng; ++gi) {
+        std::map<int, std::vector<int>> bysrc;
+        for (int sl = 0; sl < 8; ++sl) {
+            const int n = grecv[gi * 8 + sl];
+            if (n < 0) continue;
+            gslen[gi] = (int)spec_len(s, s.level[n], c->dmap.half_spectrum != 0);
+            for (int p = s.i2o_ptr[n]; p < s.i2o_ptr[n + 1]; ++p) {
+                auto &row = bysrc[s.i2o_src[p]];
+                if (row.empty()) row.assign(8, -1);
+                if (row[sl] >= 0) return H2B_OK;  // duplicate pair: keep the per-node kernel
+                const int64_t ko = cpl_elem_off[s.i2o_coupling[p]];
+                if (ko > INT32_MAX - 8192) return H2B_OK;  // offsets must fit 32 bits here
+                row[sl] = (int)ko;
+            }
+        }
+        for (auto &kv : bysrc) {
+            gsrc.push_back(other_spec_off[kv.first]);
+            gkof.insert(gkof.end(), kv.second.begin(), kv.second.end());
+        }
+        gptr.push_back((int)gsrc.size());
+    }
+    SibGroups &g = h.sib;
+    int *p;
+    int64_t *q;
+    CUDA_TRY(c->upload(&p, grecv.data(), std::max<size_t>(grecv.size(), 1))); g.recv = p;
+    CUDA_TRY(c->upload(&p, gslen.data(), std::max<size_t>(gslen.size(), 1))); g.slen = p;
+    CUDA_TRY(c->upload(&p, gptr.data(), gptr.size())); g.ptr = p;
+    CUDA_TRY(c->upload(&q, gsrc.data(), std::max<size_t>(gsrc.size(), 1))); g.src_off = q;
+    CUDA_TRY(c->upload(&p, gkof.data(), std::max<size_t>(gkof.size(), 1))); g.kof = p;
+    g.ngroups = ng;
+    for (int v : gslen) h.maxslen = std::max(h.maxslen, v);
     return H2B_OK;
 }
 
@@ -764,6 +825,10 @@ h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
         }
         CUDA_TRY(c->upload(&q, psrc.data(), psrc.size())); h.d.pair_src = q;
         CUDA_TRY(c->upload(&q, pcpl.data(), pcpl.size())); h.d.pair_cpl = q;
+        if (toep) {
+            st = build_sibling_groups(c, sd, h, o.spec_off_host, off);
+            if (st) return st;
+        }
     }
     return build_near(c, d);
 }
@@ -906,6 +971,10 @@ struct BusyGuard {
 h2b_status run_i2o(h2b_core *c, const SideHost &D, const SideHost &A, const FarArgs &fa, cudaStream_t st) {
     const int maxcoef = std::max(A.maxcoef, D.maxcoef);
     const int maxt = std::max(A.maxtsize, D.maxtsize);
+    if (D.sib.ngroups > 0) {
+        CUDA_TRY(launch_i2o_siblings(c->field == H2B_COMPLEX, c->precision, c->dmap, D.d, D.sib, D.maxslen, fa, st));
+        return H2B_OK;
+    }
     CUDA_TRY(launch_i2o(c->field == H2B_COMPLEX, c->precision, c->dmap, D.d, A.d, D.d_recv, D.n_recv, fa,
                         maxcoef, maxt, D.maxhalf, st));
     return H2B_OK;

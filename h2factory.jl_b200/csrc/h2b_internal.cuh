@@ -20,11 +20,14 @@ struct Cx {
 using cdouble = Cx<double>;
 using cfloat = Cx<float>;
 
+// Acc: the arithmetic type of every far-field sum. The FP32 form stores moments, spectra, collections,
+// transfers and couplings in FP32 (half the bytes) but accumulates in FP64, so each stored
+// intermediate is rounded once instead of once per operation.
 template <class T> struct ScalarTraits;
-template <> struct ScalarTraits<double> { using Real = double; using Complex = cdouble; static constexpr bool is_complex = false; };
-template <> struct ScalarTraits<float> { using Real = float; using Complex = cfloat; static constexpr bool is_complex = false; };
-template <> struct ScalarTraits<cdouble> { using Real = double; using Complex = cdouble; static constexpr bool is_complex = true; };
-template <> struct ScalarTraits<cfloat> { using Real = float; using Complex = cfloat; static constexpr bool is_complex = true; };
+template <> struct ScalarTraits<double> { using Real = double; using Complex = cdouble; using Acc = double; using CAcc = cdouble; static constexpr bool is_complex = false; };
+template <> struct ScalarTraits<float> { using Real = float; using Complex = cfloat; using Acc = double; using CAcc = cdouble; static constexpr bool is_complex = false; };
+template <> struct ScalarTraits<cdouble> { using Real = double; using Complex = cdouble; using Acc = cdouble; using CAcc = cdouble; static constexpr bool is_complex = true; };
+template <> struct ScalarTraits<cfloat> { using Real = float; using Complex = cfloat; using Acc = cdouble; using CAcc = cdouble; static constexpr bool is_complex = true; };
 
 template <class R> __host__ __device__ __forceinline__ Cx<R> operator+(Cx<R> a, Cx<R> b) { return {a.x + b.x, a.y + b.y}; }
 template <class R> __host__ __device__ __forceinline__ Cx<R> operator-(Cx<R> a, Cx<R> b) { return {a.x - b.x, a.y - b.y}; }
@@ -55,11 +58,22 @@ __host__ __device__ __forceinline__ double to_v(double t) { return t; }
 __host__ __device__ __forceinline__ double to_v(float t) { return (double)t; }
 __host__ __device__ __forceinline__ cdouble to_v(cdouble t) { return t; }
 __host__ __device__ __forceinline__ cdouble to_v(cfloat t) { return {(double)t.x, (double)t.y}; }
+// widening to the accumulation type and rounding back to the storage type
+__host__ __device__ __forceinline__ double wide(double a) { return a; }
+__host__ __device__ __forceinline__ double wide(float a) { return (double)a; }
+__host__ __device__ __forceinline__ cdouble wide(cdouble a) { return a; }
+__host__ __device__ __forceinline__ cdouble wide(cfloat a) { return {(double)a.x, (double)a.y}; }
+__host__ __device__ __forceinline__ void narrow(double a, double &o) { o = a; }
+__host__ __device__ __forceinline__ void narrow(double a, float &o) { o = (float)a; }
+__host__ __device__ __forceinline__ void narrow(cdouble a, cdouble &o) { o = a; }
+__host__ __device__ __forceinline__ void narrow(cdouble a, cfloat &o) { o = {(float)a.x, (float)a.y}; }
 // moment <-> spectrum
 template <class R> __host__ __device__ __forceinline__ Cx<R> to_cx(R a) { return {a, (R)0}; }
 template <class R> __host__ __device__ __forceinline__ Cx<R> to_cx(Cx<R> a) { return a; }
 template <class R> __host__ __device__ __forceinline__ void from_cx(Cx<R> s, R &out) { out = s.x; }
 template <class R> __host__ __device__ __forceinline__ void from_cx(Cx<R> s, Cx<R> &out) { out = s; }
+__host__ __device__ __forceinline__ void from_cx(cdouble s, float &out) { out = (float)s.x; }
+__host__ __device__ __forceinline__ void from_cx(cdouble s, cfloat &out) { out = {(float)s.x, (float)s.y}; }
 
 // ---------------------------------------------------------------------------------------------
 // Device-resident side of a core (all pointers device memory).
@@ -106,6 +120,16 @@ struct DNear {
     bool symmetric = false;  // N^T == N: transposed products run on `fwd`
 };
 
+// Sibling groups for the Toeplitz I2O (i2o_sibling_kernel): the receiving children of one parent.
+struct SibGroups {
+    int ngroups = 0;
+    const int *recv = nullptr;         // [ngroups*8] receiving node per child slot, -1 if none
+    const int *slen = nullptr;         // [ngroups] stored spectrum length of the group's level
+    const int *ptr = nullptr;          // [ngroups+1] into src_off / kof
+    const int64_t *src_off = nullptr;  // spectrum offset (per unit rhs) of each source of the union
+    const int *kof = nullptr;          // [nentries*8] coupling offset of (source, slot), -1 if no pair
+};
+
 // Per-call arguments of the far passes.
 struct FarArgs {
     int mode;     // H2B_FORWARD / H2B_TRANSPOSE / H2B_ADJOINT
@@ -135,6 +159,8 @@ cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &rec
 cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const DSide &s,
                                 const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
                                 int maxtsize, int maxaxis, cudaStream_t st);
+cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const DSide &recv,
+                                const SibGroups &g, int maxslen, const FarArgs &fa, cudaStream_t st);
 cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const DSide &s,
                                  const int *nodes, int nnodes, const uint8_t *received,
                                  const FarArgs &fa, int maxcoef, int maxsep, cudaStream_t st);

@@ -15,6 +15,7 @@
 // output for A^T x), so every global read is coalesced.
 
 #include <algorithm>
+#include <type_traits>
 
 #include "h2b_internal.cuh"
 
@@ -22,8 +23,6 @@ namespace h2b {
 
 namespace {
 
-constexpr int RCH = 4;   // right-hand sides per register chunk
-constexpr int JT = 64;   // x values staged in shared memory per tile
 
 __device__ __forceinline__ int ncoef_of(const DSide &s, int lvl) {
     return s.shape[3 * lvl] * s.shape[3 * lvl + 1] * s.shape[3 * lvl + 2];
@@ -36,64 +35,96 @@ __device__ __forceinline__ int sep_bound(const DSide &s, int lp) {
     return b;
 }
 
-__device__ __forceinline__ double shfl_x(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
-__device__ __forceinline__ float shfl_x(float v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
-template <class R> __device__ __forceinline__ Cx<R> shfl_x(Cx<R> v, int o) {
-    return {shfl_x(v.x, o), shfl_x(v.y, o)};
-}
-template <class T> __device__ __forceinline__ T warp_sum(T v) {
+// ---------------------------------------------------------------------------------------------
+// Per-node small products on all right-hand sides at once: acc (+)= op(M) X over a tile of at most
+// TG_M output rows and TG_Q right-hand sides. op(M)[i, k] = M[i + k*ldm] (trans = false) or
+// M[k + i*ldm] (trans = true), conjugated when cjg. M and X are staged through shared memory in
+// chunks of TG_K along k, loaded along their contiguous dimension, in the FP64 accumulation type.
+// Thread t owns outputs o = t + j*blockDim.x, (i, q) = (o % mt, o / mt).
+// ---------------------------------------------------------------------------------------------
+constexpr int TG_M = 64, TG_K = 32, TG_Q = 16, TG_LD = TG_K + 1;
+constexpr int TG_O = TG_M * TG_Q / 256;  // outputs per thread at 256 threads
+
+template <class T, class A, class XLoad>
+__device__ __forceinline__ void tile_gemm(const T *__restrict__ M, int64_t ldm, bool trans, bool cjg, int m0,
+                                          int mt, int kk, int nq, XLoad xload, A *Ms, A *Xs, A (&acc)[TG_O]) {
+    for (int k0 = 0; k0 < kk; k0 += TG_K) {
+        const int kc = min(TG_K, kk - k0);
+        __syncthreads();
+        if (trans) {
+            for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
+                const int k = idx % TG_K, i = idx / TG_K;
+                Ms[i * TG_LD + k] = k < kc ? wide(cj(M[(k0 + k) + (int64_t)(m0 + i) * ldm], cjg)) : A{};
+            }
+        } else {
+            for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
+                const int i = idx % mt, k = idx / mt;
+                Ms[i * TG_LD + k] = k < kc ? wide(cj(M[(m0 + i) + (int64_t)(k0 + k) * ldm], cjg)) : A{};
+            }
+        }
+        for (int idx = threadIdx.x; idx < TG_K * nq; idx += blockDim.x) {
+            const int k = idx % TG_K, q = idx / TG_K;
+            Xs[k * TG_Q + q] = k < kc ? xload(k0 + k, q) : A{};
+        }
+        __syncthreads();
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += shfl_x(v, o);
-    return v;
+        for (int j = 0; j < TG_O; ++j) {
+            const int o = threadIdx.x + j * blockDim.x;
+            if (o < mt * nq) {
+                const int i = o % mt, q = o / mt;
+                A sacc = acc[j];
+#pragma unroll 8
+                for (int k = 0; k < TG_K; ++k) sacc = sacc + Ms[i * TG_LD + k] * Xs[k * TG_Q + q];
+                acc[j] = sacc;
+            }
+        }
+    }
 }
 
+template <class A>
+__device__ __forceinline__ void tile_zero(A (&acc)[TG_O]) {
+#pragma unroll
+    for (int j = 0; j < TG_O; ++j) acc[j] = A{};
+}
+
+// smem for tile_gemm: Ms [TG_M][TG_LD] + Xs [TG_K][TG_Q]
+template <class A>
+constexpr size_t tile_smem() { return (size_t)(TG_M * TG_LD + TG_K * TG_Q) * sizeof(A); }
+
 // ---------------------------------------------------------------------------------------------
-// A1: m_leaf[c][r] = op(C_c) x[values]   (op = conj for adjoint maps with conjugating leaves)
+// A1: m_leaf[c][r] = op(C_c) x[values]   (op = conj for adjoint maps with conjugating leaves);
+// RCH right-hand sides share each pass over the collection
 // ---------------------------------------------------------------------------------------------
 template <class T, class V>
-__global__ void leaf_aggregate_kernel(DMap m, DSide s, const int *__restrict__ leaves, bool conjc,
-                                      int nrhs, const V *__restrict__ x, int64_t ldx,
-                                      T *__restrict__ am) {
-    __shared__ T xs[JT * RCH];
+__global__ void __launch_bounds__(256)
+leaf_aggregate_kernel(DMap m, DSide s, const int *__restrict__ leaves, bool conjc, int nrhs,
+                      const V *__restrict__ x, int64_t ldx, T *__restrict__ am) {
+    using A = typename ScalarTraits<T>::Acc;  // == V
+    extern __shared__ unsigned char smem_raw[];
+    A *Ms = reinterpret_cast<A *>(smem_raw), *Xs = Ms + TG_M * TG_LD;
     const int leaf = leaves[blockIdx.x];
     const int nc = ncoef_of(s, s.level[leaf]);
     const int v0 = s.value_ptr[leaf], nv = s.value_ptr[leaf + 1] - v0;
     const T *C = static_cast<const T *>(s.coll) + s.coll_off[leaf];
     T *mom = am + s.mom_off[leaf] * nrhs;
-    for (int c = 0; c < m.ncomp; ++c) {
-        const T *Cc = C + (int64_t)c * nc * nv;
-        for (int r0 = 0; r0 < nrhs; r0 += RCH) {
-            const int rc = min(RCH, nrhs - r0);
-            for (int a0 = 0; a0 < nc; a0 += blockDim.x) {
-                const int a = a0 + threadIdx.x;
-                T acc[RCH];
+    for (int c = 0; c < m.ncomp; ++c)
+        for (int q0 = 0; q0 < nrhs; q0 += TG_Q) {
+            const int nq = min(TG_Q, nrhs - q0);
+            for (int m0 = 0; m0 < nc; m0 += TG_M) {
+                const int mt = min(TG_M, nc - m0);
+                A acc[TG_O];
+                tile_zero(acc);
+                tile_gemm(C + (int64_t)c * nc * nv, nc, false, conjc, m0, mt, nv, nq,
+                          [&](int k, int q) -> A { return x[(int64_t)(q0 + q) * ldx + s.value[v0 + k]]; },
+                          Ms, Xs, acc);
 #pragma unroll
-                for (int q = 0; q < RCH; ++q) acc[q] = sc_zero<T>();
-                for (int j0 = 0; j0 < nv; j0 += JT) {
-                    const int jt = min(JT, nv - j0);
-                    __syncthreads();
-                    for (int e = threadIdx.x; e < JT * RCH; e += blockDim.x) {
-                        const int jj = e / RCH, q = e % RCH;
-                        xs[e] = (jj < jt && q < rc)
-                                    ? to_t(x[(int64_t)(r0 + q) * ldx + s.value[v0 + j0 + jj]], T{})
-                                    : sc_zero<T>();
-                    }
-                    __syncthreads();
-                    if (a < nc) {
-                        const T *col = Cc + (int64_t)j0 * nc + a;
-#pragma unroll 4
-                        for (int jj = 0; jj < jt; ++jj) {
-                            const T cij = cj(col[(int64_t)jj * nc], conjc);
-#pragma unroll
-                            for (int q = 0; q < RCH; ++q) acc[q] = acc[q] + cij * xs[jj * RCH + q];
-                        }
-                    }
+                for (int j = 0; j < TG_O; ++j) {
+                    const int o = threadIdx.x + j * blockDim.x;
+                    if (o < mt * nq)
+                        narrow(acc[j], mom[((int64_t)c * nrhs + q0 + o / mt) * nc + m0 + o % mt]);
                 }
-                if (a < nc)
-                    for (int q = 0; q < rc; ++q) mom[((int64_t)c * nrhs + r0 + q) * nc + a] = acc[q];
             }
         }
-    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -102,9 +133,9 @@ __global__ void leaf_aggregate_kernel(DMap m, DSide s, const int *__restrict__ l
 // `tr`, conjugated when `cjg`. Factor ax is stored sp[ax] x sc[ax] (parent x child), column-major.
 // Buffers a, b hold max(prod(fin), prod(fout)) elements; in is consumed from `a`.
 // ---------------------------------------------------------------------------------------------
-template <class T>
+template <class T, class A, class O>
 __device__ void separable_block(const T *M, const int *sp, const int *sc, int dim, bool up, bool cjg,
-                                T *a, T *b, T *out, bool accumulate) {
+                                A *a, A *b, O *out, bool accumulate) {
     int cur[3], fin[3], fout[3];
     for (int d = 0; d < 3; ++d) {
         fin[d] = up ? sc[d] : sp[d];
@@ -125,13 +156,13 @@ __device__ void separable_block(const T *M, const int *sp, const int *sc, int di
         for (int e = threadIdx.x; e < total; e += blockDim.x) {
             int idx[3] = {e % nxt[0], (e / nxt[0]) % nxt[1], e / (nxt[0] * nxt[1])};
             const int row = idx[ax];
-            T acc = sc_zero<T>();
+            A acc = sc_zero<A>();
             for (int k = 0; k < cur[ax]; ++k) {
                 int src[3] = {idx[0], idx[1], idx[2]};
                 src[ax] = k;
                 // up: op(M)[row,k] = M[row + k*ld]; down: M^T[row,k] = M[k + row*ld]
                 const T mk = up ? fac[ax][row + k * ld] : fac[ax][k + row * ld];
-                acc = acc + cj(mk, cjg) * a[src[0] + cur[0] * (src[1] + cur[1] * src[2])];
+                acc = acc + wide(cj(mk, cjg)) * a[src[0] + cur[0] * (src[1] + cur[1] * src[2])];
             }
             b[e] = acc;
         }
@@ -141,7 +172,7 @@ __device__ void separable_block(const T *M, const int *sp, const int *sc, int di
         cur[0] = nxt[0]; cur[1] = nxt[1]; cur[2] = nxt[2];
     }
     const int total = fout[0] * fout[1] * fout[2];
-    for (int e = threadIdx.x; e < total; e += blockDim.x) out[e] = accumulate ? out[e] + a[e] : a[e];
+    for (int e = threadIdx.x; e < total; e += blockDim.x) narrow(accumulate ? wide(out[e]) + a[e] : a[e], out[e]);
     __syncthreads();
 }
 
@@ -151,8 +182,9 @@ __device__ void separable_block(const T *M, const int *sp, const int *sc, int di
 template <class T>
 __global__ void transfer_up_kernel(DMap m, DSide s, const int *__restrict__ nodes, bool conjt,
                                    int nrhs, T *__restrict__ am) {
+    using A = typename ScalarTraits<T>::Acc;
     extern __shared__ unsigned char smem_raw[];
-    T *sm = reinterpret_cast<T *>(smem_raw);
+    A *sm = reinterpret_cast<A *>(smem_raw);
     const int p = nodes[blockIdx.x];
     const int lp = s.level[p], lc = lp + 1;
     const int nout = ncoef_of(s, lp), nin = ncoef_of(s, lc);
@@ -160,50 +192,43 @@ __global__ void transfer_up_kernel(DMap m, DSide s, const int *__restrict__ node
     const int c0 = s.child_ptr[p], c1 = s.child_ptr[p + 1];
     const int nq = m.ncomp * nrhs;
     if (m.transfer_kind == H2B_TRANSFER_DENSE) {
-        // children split over `ns` thread groups of `npad` threads, partial sums reduced in smem
-        const int npad = ((nout + 31) / 32) * 32;
-        const int ns = npad <= (int)blockDim.x ? (int)blockDim.x / npad : 1;
-        const int sidx = threadIdx.x / npad;
-        for (int q = 0; q < nq; ++q)
-            for (int a0 = 0; a0 < nout; a0 += (ns > 1 ? npad : (int)blockDim.x)) {
-                const int a = a0 + (ns > 1 ? (int)threadIdx.x % npad : (int)threadIdx.x);
-                T acc = sc_zero<T>();
-                if (sidx < ns && a < nout)
-                    for (int k = c0 + sidx; k < c1; k += ns) {
-                        const int ch = s.child[k];
-                        const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
-                        const T *mc = am + s.mom_off[ch] * nrhs + (int64_t)q * nin;
-#pragma unroll 4
-                        for (int b = 0; b < nin; ++b) acc = acc + cj(Tk[a + (int64_t)b * nout], conjt) * mc[b];
-                    }
-                if (ns > 1) {
-                    if (sidx < ns) sm[sidx * npad + (threadIdx.x % npad)] = acc;
-                    __syncthreads();
-                    if (threadIdx.x < npad && a0 + threadIdx.x < nout) {
-                        T sum = sm[threadIdx.x];
-                        for (int w = 1; w < ns; ++w) sum = sum + sm[w * npad + threadIdx.x];
-                        mp[(int64_t)q * nout + a0 + threadIdx.x] = sum;
-                    }
-                    __syncthreads();
-                } else if (a < nout) {
-                    mp[(int64_t)q * nout + a] = acc;
+        A *Ms = sm, *Xs = sm + TG_M * TG_LD;
+        for (int q0 = 0; q0 < nq; q0 += TG_Q) {
+            const int nqc = min(TG_Q, nq - q0);
+            for (int m0 = 0; m0 < nout; m0 += TG_M) {
+                const int mt = min(TG_M, nout - m0);
+                A acc[TG_O];
+                tile_zero(acc);
+                for (int k = c0; k < c1; ++k) {
+                    const int ch = s.child[k];
+                    const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
+                    const T *mc = am + s.mom_off[ch] * nrhs;
+                    tile_gemm(Tk, nout, false, conjt, m0, mt, nin, nqc,
+                              [&](int kk, int q) -> A { return wide(mc[(int64_t)(q0 + q) * nin + kk]); }, Ms, Xs,
+                              acc);
+                }
+#pragma unroll
+                for (int j = 0; j < TG_O; ++j) {
+                    const int o = threadIdx.x + j * blockDim.x;
+                    if (o < mt * nqc) narrow(acc[j], mp[(int64_t)(q0 + o / mt) * nout + m0 + o % mt]);
                 }
             }
+        }
         return;
     }
     const int mx = sep_bound(s, lp);
-    T *bufa = sm, *bufb = sm + mx, *acc = sm + 2 * mx;
+    A *bufa = sm, *bufb = sm + mx, *acc = sm + 2 * mx;
     for (int q = 0; q < nq; ++q) {
         for (int k = c0; k < c1; ++k) {
             const int ch = s.child[k];
             const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
             const T *mc = am + s.mom_off[ch] * nrhs + (int64_t)q * nin;
-            for (int e = threadIdx.x; e < nin; e += blockDim.x) bufa[e] = mc[e];
+            for (int e = threadIdx.x; e < nin; e += blockDim.x) bufa[e] = wide(mc[e]);
             __syncthreads();
             separable_block(Tk, &s.shape[3 * lp], &s.shape[3 * lc], m.dim, true, conjt, bufa, bufb,
                             acc, k != c0);
         }
-        for (int e = threadIdx.x; e < nout; e += blockDim.x) mp[(int64_t)q * nout + e] = acc[e];
+        for (int e = threadIdx.x; e < nout; e += blockDim.x) narrow(acc[e], mp[(int64_t)q * nout + e]);
         __syncthreads();
     }
 }
@@ -315,12 +340,12 @@ template <class T, int NMAX>
 __global__ void __launch_bounds__(256) toeplitz_in_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
                                    int nrhs, int maxt, const T *__restrict__ am,
                                    typename ScalarTraits<T>::Complex *__restrict__ as) {
-    using S = typename ScalarTraits<T>::Complex;
-    using R = typename ScalarTraits<T>::Real;
+    using S = typename ScalarTraits<T>::Complex;  // stored spectra
+    using W = cdouble;                             // transforms run in FP64
     extern __shared__ unsigned char smem_raw[];
     const int grp = threadIdx.x / FFT_T, tl = threadIdx.x % FFT_T, ngrp = blockDim.x / FFT_T;
-    S *a = reinterpret_cast<S *>(smem_raw) + (size_t)grp * (maxt + 3 * FFT_NMAX);
-    S *tw = a + maxt;
+    W *a = reinterpret_cast<W *>(smem_raw) + (size_t)grp * (maxt + 3 * FFT_NMAX);
+    W *tw = a + maxt;
     const int nq = m.ncomp * nrhs;
     const int t = blockIdx.x * ngrp + grp;
     const bool busy = t < ntrans;
@@ -331,18 +356,18 @@ __global__ void __launch_bounds__(256) toeplitz_in_kernel(DMap m, DSide s, const
         const T *mom = am + s.mom_off[node] * nrhs + (int64_t)q * g.nc;
         for (int e = tl; e < g.nt; e += FFT_T) {
             const int i1 = e % g.ts[0], i2 = (e / g.ts[0]) % g.ts[1], i3 = e / (g.ts[0] * g.ts[1]);
-            S v = {(R)0, (R)0};
+            W v = {0.0, 0.0};
             if (i1 < g.sh[0] && i2 < g.sh[1] && i3 < g.sh[2])
-                v = to_cx(mom[i1 + g.sh[0] * (i2 + g.sh[1] * i3)]);
+                v = to_cx(wide(mom[i1 + g.sh[0] * (i2 + g.sh[1] * i3)]));
             a[e] = v;
         }
     }
-    dft_group<R, NMAX>(a, g, inverse, tw, tl, busy);
+    dft_group<double, NMAX>(a, g, inverse, tw, tl, busy);
     if (busy) {
         S *spec = as + s.spec_off[node] * nrhs + (int64_t)q * g.slen;
         for (int e = tl; e < g.slen; e += FFT_T) {
             const int k1 = e % g.h0, r = e / g.h0;
-            spec[e] = a[k1 + g.ts[0] * r];
+            narrow(a[k1 + g.ts[0] * r], spec[e]);
         }
     }
 }
@@ -353,12 +378,12 @@ __global__ void __launch_bounds__(256) toeplitz_out_kernel(DMap m, DSide s, cons
                                     int nrhs, int maxt,
                                     const typename ScalarTraits<T>::Complex *__restrict__ ds,
                                     T *__restrict__ dm) {
-    using S = typename ScalarTraits<T>::Complex;
-    using R = typename ScalarTraits<T>::Real;
+    using S = typename ScalarTraits<T>::Complex;  // stored spectra
+    using W = cdouble;                             // transforms run in FP64
     extern __shared__ unsigned char smem_raw[];
     const int grp = threadIdx.x / FFT_T, tl = threadIdx.x % FFT_T, ngrp = blockDim.x / FFT_T;
-    S *a = reinterpret_cast<S *>(smem_raw) + (size_t)grp * (maxt + 3 * FFT_NMAX);
-    S *tw = a + maxt;
+    W *a = reinterpret_cast<W *>(smem_raw) + (size_t)grp * (maxt + 3 * FFT_NMAX);
+    W *tw = a + maxt;
     const int nq = m.ncomp * nrhs;
     const int t = blockIdx.x * ngrp + grp;
     const bool busy = t < ntrans;
@@ -370,15 +395,15 @@ __global__ void __launch_bounds__(256) toeplitz_out_kernel(DMap m, DSide s, cons
         for (int e = tl; e < g.nt; e += FFT_T) {
             const int k1 = e % g.ts[0], r = e / g.ts[0];
             if (k1 < g.h0) {
-                a[e] = spec[k1 + g.h0 * r];
+                a[e] = wide(spec[k1 + g.h0 * r]);
             } else {
                 const int k2 = r % g.ts[1], k3 = r / g.ts[1];
                 const int m1 = g.ts[0] - k1, m2 = (g.ts[1] - k2) % g.ts[1], m3 = (g.ts[2] - k3) % g.ts[2];
-                a[e] = conjg(spec[m1 + g.h0 * (m2 + g.ts[1] * m3)]);
+                a[e] = conjg(wide(spec[m1 + g.h0 * (m2 + g.ts[1] * m3)]));
             }
         }
     }
-    dft_group<R, NMAX>(a, g, inverse, tw, tl, busy);
+    dft_group<double, NMAX>(a, g, inverse, tw, tl, busy);
     if (busy) {
         T *mom = dm + s.mom_off[node] * nrhs + (int64_t)q * g.nc;
         for (int e = tl; e < g.nc; e += FFT_T) {
@@ -395,11 +420,12 @@ __global__ void __launch_bounds__(256) toeplitz_out_kernel(DMap m, DSide s, cons
 // toeplitzi2ocollection.jl:110-193). The first pair overwrites.
 // ---------------------------------------------------------------------------------------------
 template <class T>
-__global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mode,
+__global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mode,
                            int nrhs, const T *__restrict__ am, T *__restrict__ dm,
                            const typename ScalarTraits<T>::Complex *__restrict__ as,
                            typename ScalarTraits<T>::Complex *__restrict__ ds) {
     using S = typename ScalarTraits<T>::Complex;
+    using A = typename ScalarTraits<T>::Acc;
     const int node = nodes[blockIdx.x];
     const int p0 = r.i2o_ptr[node], p1 = r.i2o_ptr[node + 1];
     const int lvl = r.level[node];
@@ -409,27 +435,48 @@ __global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nod
     // r.pair_src[p]: the source's moment (or spectrum) offset per unit rhs; r.pair_cpl[p]: the
     // coupling's element offset -- one load each per pair, no chained index lookups
     if (m.coupling_kind == H2B_COUPLING_TOEPLITZ) {
+        // each kernel value is loaded once and applied to up to QB right-hand sides
+        constexpr int QB = 8;
         const int nt = tgeom(r, lvl, m.half_spectrum != 0).slen;
         S *out = ds + r.spec_off[node] * nrhs;
         const S *K0 = static_cast<const S *>(m.cpl);
-        for (int q = 0; q < nq; ++q)
+        for (int q0 = 0; q0 < nq; q0 += QB) {
+            const int qc = min(QB, nq - q0);
             for (int e = threadIdx.x; e < nt; e += blockDim.x) {
-                S acc = {0, 0};
-                int p = p0;
-                for (; p + 4 <= p1; p += 4) {
-                    S kv[4], iv[4];
+                if (qc == 1) {
+                    cdouble acc = {0.0, 0.0};
+                    int p = p0;
+                    for (; p + 4 <= p1; p += 4) {
+                        S kv[4], iv[4];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        kv[u] = K0[r.pair_cpl[p + u] + e];
-                        iv[u] = as[r.pair_src[p + u] * nrhs + (int64_t)q * nt + e];
+                        for (int u = 0; u < 4; ++u) {
+                            kv[u] = K0[r.pair_cpl[p + u] + e];
+                            iv[u] = as[r.pair_src[p + u] * nrhs + (int64_t)q0 * nt + e];
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) acc = acc + wide(cj(kv[u], adj)) * wide(iv[u]);
+                    }
+                    for (; p < p1; ++p)
+                        acc = acc + wide(cj(K0[r.pair_cpl[p] + e], adj)) *
+                                        wide(as[r.pair_src[p] * nrhs + (int64_t)q0 * nt + e]);
+                    narrow(acc, out[(int64_t)q0 * nt + e]);
+                } else {
+                    cdouble acc[QB];
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) acc[q] = cdouble{0.0, 0.0};
+                    for (int p = p0; p < p1; ++p) {
+                        const cdouble kv = wide(cj(K0[r.pair_cpl[p] + e], adj));
+                        const S *in = as + r.pair_src[p] * nrhs + (int64_t)q0 * nt + e;
+#pragma unroll
+                        for (int q = 0; q < QB; ++q)
+                            if (q < qc) acc[q] = acc[q] + kv * wide(in[(int64_t)q * nt]);
                     }
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) acc = acc + cj(kv[u], adj) * iv[u];
+                    for (int q = 0; q < QB; ++q)
+                        if (q < qc) narrow(acc[q], out[(int64_t)(q0 + q) * nt + e]);
                 }
-                for (; p < p1; ++p)
-                    acc = acc + cj(K0[r.pair_cpl[p] + e], adj) * as[r.pair_src[p] * nrhs + (int64_t)q * nt + e];
-                out[(int64_t)q * nt + e] = acc;
             }
+        }
         return;
     }
     T *out = dm + r.mom_off[node] * nrhs;
@@ -437,44 +484,110 @@ __global__ void i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nod
     if (m.coupling_kind == H2B_COUPLING_DIAGONAL) {
         for (int q = 0; q < nq; ++q)
             for (int a = threadIdx.x; a < nc; a += blockDim.x) {
-                T acc = sc_zero<T>();
+                A acc = sc_zero<A>();
                 for (int p = p0; p < p1; ++p) {
                     const T *D = B0 + r.pair_cpl[p];
-                    acc = acc + cj(D[a], adj) * am[r.pair_src[p] * nrhs + (int64_t)q * nc + a];
+                    acc = acc + wide(cj(D[a], adj)) * wide(am[r.pair_src[p] * nrhs + (int64_t)q * nc + a]);
                 }
-                out[(int64_t)q * nc + a] = acc;
+                narrow(acc, out[(int64_t)q * nc + a]);
             }
         return;
     }
-    if (mode == H2B_FORWARD) {
-        // thread per output row: B[a + b*nc] coalesced over a
-        for (int q = 0; q < nq; ++q)
-            for (int a = threadIdx.x; a < nc; a += blockDim.x) {
-                T acc = sc_zero<T>();
-                for (int p = p0; p < p1; ++p) {
-                    const int snc = ncoef_of(t, t.level[r.i2o_src[p]]);
-                    const T *B = B0 + r.pair_cpl[p];
-                    const T *in = am + r.pair_src[p] * nrhs + (int64_t)q * snc;
-                    for (int b = 0; b < snc; ++b) acc = acc + B[a + (int64_t)b * nc] * in[b];
-                }
-                out[(int64_t)q * nc + a] = acc;
-            }
-        return;
-    }
-    // transpose / adjoint: output a is column a of the stored block -> warp per output
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int q = 0; q < nq; ++q)
-        for (int a = warp; a < nc; a += nw) {
-            T acc = sc_zero<T>();
+    // dense: out (nc x nq) = sum over pairs of op(B) X_src, all right-hand sides per pass
+    extern __shared__ unsigned char smem_raw[];
+    A *Ms = reinterpret_cast<A *>(smem_raw), *Xs = Ms + TG_M * TG_LD;
+    for (int q0 = 0; q0 < nq; q0 += TG_Q) {
+        const int nqc = min(TG_Q, nq - q0);
+        for (int m0 = 0; m0 < nc; m0 += TG_M) {
+            const int mt = min(TG_M, nc - m0);
+            A acc[TG_O];
+            tile_zero(acc);
             for (int p = p0; p < p1; ++p) {
                 const int snc = ncoef_of(t, t.level[r.i2o_src[p]]);
-                const T *B = B0 + r.pair_cpl[p] + (int64_t)a * snc;
-                const T *in = am + r.pair_src[p] * nrhs + (int64_t)q * snc;
-                for (int b = lane; b < snc; b += 32) acc = acc + cj(B[b], adj) * in[b];
+                const T *B = B0 + r.pair_cpl[p];
+                const T *X = am + r.pair_src[p] * nrhs;
+                // forward: block (r, t) is nc x snc; transposed: block (t, r) is snc x nc
+                tile_gemm(B, mode == H2B_FORWARD ? nc : snc, mode != H2B_FORWARD, adj, m0, mt, snc, nqc,
+                          [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + k]); }, Ms, Xs, acc);
             }
-            acc = warp_sum(acc);
-            if (lane == 0) out[(int64_t)q * nc + a] = acc;
+#pragma unroll
+            for (int j = 0; j < TG_O; ++j) {
+                const int o = threadIdx.x + j * blockDim.x;
+                if (o < mt * nqc) narrow(acc[j], out[(int64_t)(q0 + o / mt) * nc + m0 + o % mt]);
+            }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// B2 by sibling groups: the Toeplitz I2O of the receiving children of one parent together. One CTA
+// per (group, block of right-hand sides), one thread per stored frequency. The CTA walks the union
+// of the siblings' sources once; each source spectrum value is loaded once and applied from
+// registers to every sibling translating from it, with that pair's kernel value (loaded through
+// L1). Per complex multiply-add this moves one kernel value per QB right-hand sides and one source
+// value per group instead of one of each per pair.
+// ---------------------------------------------------------------------------------------------
+template <class T, int QB>
+__global__ void __launch_bounds__(512)
+i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
+                   const typename ScalarTraits<T>::Complex *__restrict__ as,
+                   typename ScalarTraits<T>::Complex *__restrict__ ds) {
+    using S = typename ScalarTraits<T>::Complex;
+    const int gi = blockIdx.x;
+    const int q0 = blockIdx.y * QB;
+    const int nq = m.ncomp * nrhs;
+    const int e = threadIdx.x;
+    const int slen = g.slen[gi];
+    if (e >= slen) return;  // no barriers below
+    const bool adj = mode == H2B_ADJOINT;
+    const S *K0 = static_cast<const S *>(m.cpl);
+    const int k0 = g.ptr[gi], k1 = g.ptr[gi + 1];
+    cdouble acc[8][QB];
+#pragma unroll
+    for (int sl = 0; sl < 8; ++sl)
+#pragma unroll
+        for (int q = 0; q < QB; ++q) acc[sl][q] = cdouble{0.0, 0.0};
+    // U source entries per step (two for one right-hand side, where registers allow), every load
+    // issued before the arithmetic that uses it
+    constexpr int U = QB == 1 ? 2 : 1;
+    for (int k = k0; k < k1; k += U) {
+        cdouble sv[U][QB];
+        int ko[U][8];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool ok = k + u < k1;
+            const int *kof = g.kof + (int64_t)(ok ? k + u : k) * 8;
+#pragma unroll
+            for (int sl = 0; sl < 8; ++sl) ko[u][sl] = ok ? kof[sl] : -1;
+            const S *sp = as + g.src_off[ok ? k + u : k] * nrhs + (int64_t)q0 * slen + e;
+#pragma unroll
+            for (int q = 0; q < QB; ++q) sv[u][q] = q0 + q < nq ? wide(sp[(int64_t)q * slen]) : cdouble{0.0, 0.0};
+        }
+        S kvs[U][8];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int sl = 0; sl < 8; ++sl) kvs[u][sl] = ko[u][sl] >= 0 ? K0[ko[u][sl] + e] : S{};
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int sl = 0; sl < 8; ++sl) {
+                if (ko[u][sl] >= 0) {
+                    const cdouble kv = wide(cj(kvs[u][sl], adj));
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) acc[sl][q] = acc[sl][q] + kv * sv[u][q];
+                }
+            }
+    }
+#pragma unroll
+    for (int sl = 0; sl < 8; ++sl) {
+        const int rv = g.recv[gi * 8 + sl];
+        if (rv < 0) continue;
+        S *out = ds + r.spec_off[rv] * nrhs + (int64_t)q0 * slen + e;
+#pragma unroll
+        for (int q = 0; q < QB; ++q)
+            if (q0 + q < nq) narrow(acc[sl][q], out[(int64_t)q * slen]);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -484,8 +597,9 @@ template <class T>
 __global__ void transfer_down_kernel(DMap m, DSide s, const int *__restrict__ nodes,
                                      const uint8_t *__restrict__ received, bool conjt, int nrhs,
                                      T *__restrict__ dm) {
+    using A = typename ScalarTraits<T>::Acc;
     extern __shared__ unsigned char smem_raw[];
-    T *sm = reinterpret_cast<T *>(smem_raw);
+    A *sm = reinterpret_cast<A *>(smem_raw);
     const int c = nodes[blockIdx.x];
     const int lc = s.level[c], lp = lc - 1;
     const int par = s.parent[c];
@@ -496,26 +610,32 @@ __global__ void transfer_down_kernel(DMap m, DSide s, const int *__restrict__ no
     const T *mp = dm + s.mom_off[par] * nrhs;
     const int nq = m.ncomp * nrhs;
     if (m.transfer_kind == H2B_TRANSFER_DENSE) {
-        // stored T is nin x nout (parent x child); output a reads column a: warp per output
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        for (int q = 0; q < nq; ++q)
-            for (int a = warp; a < nout; a += nw) {
-                T acc = sc_zero<T>();
-                const T *col = Tk + (int64_t)a * nin;
-                const T *in = mp + (int64_t)q * nin;
-                for (int b = lane; b < nin; b += 32) acc = acc + cj(col[b], conjt) * in[b];
-                acc = warp_sum(acc);
-                if (lane == 0) {
-                    T *o = &mc[(int64_t)q * nout + a];
-                    *o = acc0 ? *o + acc : acc;
+        // stored T is nin x nout (parent x child): op(T) = T^T (or T^H), column-contiguous in k
+        A *Ms = sm, *Xs = sm + TG_M * TG_LD;
+        for (int q0 = 0; q0 < nq; q0 += TG_Q) {
+            const int nqc = min(TG_Q, nq - q0);
+            for (int m0 = 0; m0 < nout; m0 += TG_M) {
+                const int mt = min(TG_M, nout - m0);
+                A acc[TG_O];
+                tile_zero(acc);
+                tile_gemm(Tk, nin, true, conjt, m0, mt, nin, nqc,
+                          [&](int kk, int q) -> A { return wide(mp[(int64_t)(q0 + q) * nin + kk]); }, Ms, Xs, acc);
+#pragma unroll
+                for (int j = 0; j < TG_O; ++j) {
+                    const int o = threadIdx.x + j * blockDim.x;
+                    if (o < mt * nqc) {
+                        T *dst = &mc[(int64_t)(q0 + o / mt) * nout + m0 + o % mt];
+                        narrow(acc0 ? wide(*dst) + acc[j] : acc[j], *dst);
+                    }
                 }
             }
+        }
         return;
     }
     const int mx = sep_bound(s, lp);
-    T *bufa = sm, *bufb = sm + mx;
+    A *bufa = sm, *bufb = sm + mx;
     for (int q = 0; q < nq; ++q) {
-        for (int e = threadIdx.x; e < nin; e += blockDim.x) bufa[e] = mp[(int64_t)q * nin + e];
+        for (int e = threadIdx.x; e < nin; e += blockDim.x) bufa[e] = wide(mp[(int64_t)q * nin + e]);
         __syncthreads();
         separable_block(Tk, &s.shape[3 * lp], &s.shape[3 * lc], m.dim, false, conjt, bufa, bufb,
                         mc + (int64_t)q * nout, acc0);
@@ -526,28 +646,36 @@ __global__ void transfer_down_kernel(DMap m, DSide s, const int *__restrict__ no
 // C2: y[values] = alpha * sum_c op(C_c)^T l_c + beta * y[values]  (beta == 0 overwrites)
 // ---------------------------------------------------------------------------------------------
 template <class T, class V>
-__global__ void leaf_disaggregate_kernel(DMap m, DSide s, const int *__restrict__ leaves, bool conjc,
-                                         int nrhs, const T *__restrict__ dm, V alpha, V beta,
-                                         bool beta_zero, V *__restrict__ y, int64_t ldy) {
+__global__ void __launch_bounds__(256)
+leaf_disaggregate_kernel(DMap m, DSide s, const int *__restrict__ leaves, bool conjc, int nrhs,
+                         const T *__restrict__ dm, V alpha, V beta, bool beta_zero, V *__restrict__ y,
+                         int64_t ldy) {
+    using A = typename ScalarTraits<T>::Acc;  // == V
+    extern __shared__ unsigned char smem_raw[];
+    A *Ms = reinterpret_cast<A *>(smem_raw), *Xs = Ms + TG_M * TG_LD;
     const int leaf = leaves[blockIdx.x];
     const int nc = ncoef_of(s, s.level[leaf]);
     const int v0 = s.value_ptr[leaf], nv = s.value_ptr[leaf + 1] - v0;
     const T *C = static_cast<const T *>(s.coll) + s.coll_off[leaf];
     const T *mom = dm + s.mom_off[leaf] * nrhs;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int j = warp; j < nv; j += nw) {
-        for (int r = 0; r < nrhs; ++r) {
-            T acc = sc_zero<T>();
-            for (int c = 0; c < m.ncomp; ++c) {
-                const T *col = C + (int64_t)c * nc * nv + (int64_t)j * nc;
-                const T *l = mom + ((int64_t)c * nrhs + r) * nc;
-                for (int a = lane; a < nc; a += 32) acc = acc + cj(col[a], conjc) * l[a];
-            }
-            acc = warp_sum(acc);
-            if (lane == 0) {
-                V *o = &y[(int64_t)r * ldy + s.value[v0 + j]];
-                const V v = alpha * to_v(acc);
-                *o = beta_zero ? v : v + beta * *o;
+    for (int q0 = 0; q0 < nrhs; q0 += TG_Q) {
+        const int nq = min(TG_Q, nrhs - q0);
+        for (int m0 = 0; m0 < nv; m0 += TG_M) {
+            const int mt = min(TG_M, nv - m0);
+            A acc[TG_O];
+            tile_zero(acc);
+            for (int c = 0; c < m.ncomp; ++c)
+                tile_gemm(C + (int64_t)c * nc * nv, nc, true, conjc, m0, mt, nc, nq,
+                          [&](int k, int q) -> A { return wide(mom[((int64_t)c * nrhs + q0 + q) * nc + k]); },
+                          Ms, Xs, acc);
+#pragma unroll
+            for (int j = 0; j < TG_O; ++j) {
+                const int o = threadIdx.x + j * blockDim.x;
+                if (o < mt * nq) {
+                    V *dst = &y[(int64_t)(q0 + o / mt) * ldy + s.value[v0 + m0 + o % mt]];
+                    const V v = alpha * acc[j];
+                    *dst = beta_zero ? v : v + beta * *dst;
+                }
             }
         }
     }
@@ -599,15 +727,15 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 cudaError_t launch_leaf_aggregate(bool cplx, int precision, const DMap &m, const DSide &s,
                                   const int *leaves, int nleaves, int maxcoef, bool conjc,
                                   const FarArgs &fa, const void *x, int64_t ldx, cudaStream_t st) {
+    (void)maxcoef;
     if (nleaves == 0) return cudaSuccess;
-    const int bs = block_for(maxcoef, 64, 256);
     if (!cplx) {
         H2B_DISPATCH_REAL(precision,
-            leaf_aggregate_kernel<T, double><<<nleaves, bs, 0, st>>>(
+            leaf_aggregate_kernel<T, double><<<nleaves, 256, tile_smem<double>(), st>>>(
                 m, s, leaves, conjc, fa.nrhs, static_cast<const double *>(x), ldx, static_cast<T *>(fa.am)));
     } else {
         H2B_DISPATCH_CPLX(precision,
-            leaf_aggregate_kernel<T, cdouble><<<nleaves, bs, 0, st>>>(
+            leaf_aggregate_kernel<T, cdouble><<<nleaves, 256, tile_smem<cdouble>(), st>>>(
                 m, s, leaves, conjc, fa.nrhs, static_cast<const cdouble *>(x), ldx, static_cast<T *>(fa.am)));
     }
     return cudaGetLastError();
@@ -620,8 +748,9 @@ cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DS
     const int bs = m.transfer_kind == H2B_TRANSFER_DENSE ? 256 : block_for(maxcoef);
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
-        const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? (size_t)bs * sizeof(T)
-                                                                 : 3 * (size_t)maxsep * sizeof(T);
+        using A = typename ScalarTraits<T>::Acc;
+        const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? tile_smem<A>()
+                                                                 : 3 * (size_t)maxsep * sizeof(A);
         err = allow_smem(transfer_up_kernel<T>, sm);
         if (err == cudaSuccess)
             transfer_up_kernel<T><<<nnodes, bs, sm, st>>>(m, s, nodes, conjt, fa.nrhs, static_cast<T *>(fa.am));
@@ -644,8 +773,8 @@ cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DS
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
-        const int G = fft_groups(maxtsize, sizeof(S));
-        const size_t sm = (size_t)G * (maxtsize + 3 * FFT_NMAX) * sizeof(S);
+        const int G = fft_groups(maxtsize, sizeof(cdouble));
+        const size_t sm = (size_t)G * (maxtsize + 3 * FFT_NMAX) * sizeof(cdouble);
         const int ntrans = nnodes * m.ncomp * fa.nrhs;
         auto launch = [&](auto kern) {
             cudaError_t e2 = allow_smem(kern, sm);
@@ -669,8 +798,8 @@ cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const D
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
-        const int G = fft_groups(maxtsize, sizeof(S));
-        const size_t sm = (size_t)G * (maxtsize + 3 * FFT_NMAX) * sizeof(S);
+        const int G = fft_groups(maxtsize, sizeof(cdouble));
+        const size_t sm = (size_t)G * (maxtsize + 3 * FFT_NMAX) * sizeof(cdouble);
         const int ntrans = nnodes * m.ncomp * fa.nrhs;
         auto launch = [&](auto kern) {
             cudaError_t e2 = allow_smem(kern, sm);
@@ -691,15 +820,35 @@ cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &rec
                        const DSide &src, const int *nodes, int nnodes, const FarArgs &fa,
                        int maxcoef, int maxtsize, int maxhalf, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
-    // Toeplitz: one thread per stored frequency (half spectra hold (n1/2 + 1) * n2 * n3 of them)
-    const int bs = m.coupling_kind == H2B_COUPLING_TOEPLITZ
-                       ? block_for(m.half_spectrum ? maxhalf : maxtsize, 32, 512)
-                       : block_for(maxcoef, 64, 256);
+    // Toeplitz: one thread per stored frequency (half spectra hold (n1/2 + 1) * n2 * n3 of them);
+    // dense: the tile product's 256 threads
+    const bool toep = m.coupling_kind == H2B_COUPLING_TOEPLITZ;
+    const bool diag = m.coupling_kind == H2B_COUPLING_DIAGONAL;
+    const int bs = toep ? block_for(m.half_spectrum ? maxhalf : maxtsize, 32, 512)
+                        : (diag ? block_for(maxcoef, 64, 256) : 256);
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
-        i2o_kernel<T><<<nnodes, bs, 0, st>>>(m, recv, src, nodes, fa.mode, fa.nrhs,
-                                             static_cast<const T *>(fa.am), static_cast<T *>(fa.dm),
-                                             static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
+        const size_t sm = (toep || diag) ? 0 : tile_smem<typename ScalarTraits<T>::Acc>();
+        i2o_kernel<T><<<nnodes, bs, sm, st>>>(m, recv, src, nodes, fa.mode, fa.nrhs,
+                                              static_cast<const T *>(fa.am), static_cast<T *>(fa.dm),
+                                              static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
+    });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const DSide &recv,
+                                const SibGroups &g, int maxslen, const FarArgs &fa, cudaStream_t st) {
+    if (g.ngroups == 0) return cudaSuccess;
+    const int nq = m.ncomp * fa.nrhs;
+    const int bs = block_for(maxslen, 32, 512);
+    H2B_DISPATCH_T(cplx, precision, {
+        using S = typename ScalarTraits<T>::Complex;
+        if (nq == 1)
+            i2o_sibling_kernel<T, 1><<<dim3(g.ngroups, 1), bs, 0, st>>>(
+                m, recv, g, fa.mode, fa.nrhs, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
+        else
+            i2o_sibling_kernel<T, 2><<<dim3(g.ngroups, (nq + 1) / 2), bs, 0, st>>>(
+                m, recv, g, fa.mode, fa.nrhs, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
     });
     return cudaGetLastError();
 }
@@ -708,11 +857,13 @@ cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const 
                                  const int *nodes, int nnodes, const uint8_t *received,
                                  const FarArgs &fa, int maxcoef, int maxsep, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
-    const int bs = block_for(maxcoef, 64, 256);
+    const int bs = m.transfer_kind == H2B_TRANSFER_DENSE ? 256 : block_for(maxcoef, 64, 256);
     const bool conjt = fa.mode == H2B_ADJOINT;
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
-        const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? 0 : 2 * (size_t)maxsep * sizeof(T);
+        using A = typename ScalarTraits<T>::Acc;
+        const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? tile_smem<A>()
+                                                                 : 2 * (size_t)maxsep * sizeof(A);
         err = allow_smem(transfer_down_kernel<T>, sm);
         if (err == cudaSuccess)
             transfer_down_kernel<T><<<nnodes, bs, sm, st>>>(m, s, nodes, received, conjt, fa.nrhs,
@@ -726,17 +877,17 @@ cudaError_t launch_leaf_disaggregate(bool cplx, int precision, const DMap &m, co
                                      cdouble alpha, cdouble beta, void *y, int64_t ldy,
                                      cudaStream_t st) {
     if (nleaves == 0) return cudaSuccess;
-    const int bs = 128;
+    const int bs = 256;
     if (!cplx) {
         const bool bz = beta.x == 0.0;
         H2B_DISPATCH_REAL(precision,
-            leaf_disaggregate_kernel<T, double><<<nleaves, bs, 0, st>>>(
+            leaf_disaggregate_kernel<T, double><<<nleaves, bs, tile_smem<double>(), st>>>(
                 m, s, leaves, conjc, fa.nrhs, static_cast<const T *>(fa.dm), alpha.x, beta.x, bz,
                 static_cast<double *>(y), ldy));
     } else {
         const bool bz = beta.x == 0.0 && beta.y == 0.0;
         H2B_DISPATCH_CPLX(precision,
-            leaf_disaggregate_kernel<T, cdouble><<<nleaves, bs, 0, st>>>(
+            leaf_disaggregate_kernel<T, cdouble><<<nleaves, bs, tile_smem<cdouble>(), st>>>(
                 m, s, leaves, conjc, fa.nrhs, static_cast<const T *>(fa.dm), alpha, beta, bz,
                 static_cast<cdouble *>(y), ldy));
     }

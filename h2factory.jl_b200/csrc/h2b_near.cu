@@ -3,12 +3,13 @@
 // Layout in HBM: every dense block of a (output leaf, input leaf) pair is stored column-major with
 // an even leading dimension for real fields, so that each lane of a warp streams two consecutive
 // rows with one 16-byte load. The blocks of one output leaf are split across the warps of one CTA;
-// every warp sweeps its blocks column by column with x broadcast from registers by shuffles, and
+// every warp sweeps its blocks column by column with x broadcast from shared memory, and
 // the warps' partial rows are summed in shared memory at the end. Transposed and adjoint products
 // run the same kernel on the transposed operator: N itself when N^T == N (checked once on the
 // device when the core is built), otherwise a transposed copy of the blocks built at upload.
 
 #include <algorithm>
+#include <type_traits>
 
 #include "h2b_internal.cuh"
 
@@ -25,11 +26,6 @@ template <> struct NearVec<double> {
 template <> struct NearVec<cdouble> {
     static constexpr int RPL = 1;
 };
-
-__device__ __forceinline__ double shfl_idx(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
-__device__ __forceinline__ cdouble shfl_idx(cdouble v, int src) {
-    return {__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
-}
 
 // streaming (evict-first) loads of the near blocks: they are read once per product
 __device__ __forceinline__ void load_rows(const double *p, double (&v)[2]) {
@@ -49,27 +45,47 @@ __device__ __forceinline__ cdouble fma_c(cdouble a, cdouble b, cdouble c, bool c
     return {fma(a.x, b.x, fma(-ay, b.y, c.x)), fma(a.x, b.y, fma(ay, b.x, c.y))};
 }
 
+// R x values of one column from shared memory, two per 16-byte load where the type allows
+template <class V, int R>
+__device__ __forceinline__ void load_x(const V *p, V (&v)[R]) {
+    if constexpr (sizeof(V) == 8 && R % 2 == 0) {
+#pragma unroll
+        for (int q = 0; q < R; q += 2) {
+            const double2 t = *reinterpret_cast<const double2 *>(p + q);
+            v[q] = t.x;
+            v[q + 1] = t.y;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = p[q];
+    }
+}
+
 __device__ __forceinline__ int near_ld(int nr, double *) { return nr + (nr & 1); }
 __device__ __forceinline__ int near_ld(int nr, cdouble *) { return nr; }
 
-// y[rows(g)] = alpha * op(N_g) x + beta * y[rows(g)] for right-hand sides [r0, r0 + R)
+// y[rows(g)] = alpha * op(N_g) x + beta * y[rows(g)] for right-hand sides [r0, r0 + R).
+// Shared memory: per warp, the x values of its current 32-column chunk ([32][R]), read back as
+// broadcasts; then the warps' partial rows ([NEAR_WARPS][RPP][R]) for the final reduction.
 template <class V, int R>
-__global__ void __launch_bounds__(NEAR_WARPS * 32)
+__global__ void __launch_bounds__(NEAR_WARPS * 32, 2)
 near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, const V *__restrict__ x,
                  int64_t ldx, V *__restrict__ y, int64_t ldy, V alpha, V beta, bool beta_zero) {
     constexpr int RPL = NearVec<V>::RPL;
     constexpr int RPP = 32 * RPL;  // rows per pass
     extern __shared__ unsigned char smem_raw[];
-    V *part = reinterpret_cast<V *>(smem_raw);  // [NEAR_WARPS][RPP][R]
     const int g = blockIdx.x;
     const int leaf = op.grp_leaf[g];
     const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
     const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    V *xs = reinterpret_cast<V *>(smem_raw) + warp * 32 * R;                 // this warp's x chunk
+    V *part = reinterpret_cast<V *>(smem_raw) + NEAR_WARPS * 32 * R;         // partial rows
     const V *D = static_cast<const V *>(op.data);
     const int ld = near_ld(nr, (V *)nullptr);
     for (int p0 = 0; p0 < nr; p0 += RPP) {
         const int i0 = p0 + RPL * lane;  // first row of this lane
+        const bool live = i0 < nr;       // lanes past the last row load nothing
         V acc[RPL][R];
 #pragma unroll
         for (int k = 0; k < RPL; ++k)
@@ -84,18 +100,16 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
             const V *B = D + op.blk_off[blk] + i0;
             for (int j0 = 0; j0 < nc; j0 += 32, ++unit) {
                 if (unit % NEAR_WARPS != warp) continue;
-                V xr[R];
-                const int jl = j0 + lane;
-                if (jl < nc) {
-                    const int dof = ins.value[c0 + jl];
+                __syncwarp();
+                {
+                    const int jl = j0 + lane;
+                    const int dof = jl < nc ? ins.value[c0 + jl] : 0;
 #pragma unroll
-                    for (int q = 0; q < R; ++q) xr[q] = q < rc ? x[(int64_t)(r0 + q) * ldx + dof] : V{};
-                } else {
-#pragma unroll
-                    for (int q = 0; q < R; ++q) xr[q] = V{};
+                    for (int q = 0; q < R; ++q)
+                        xs[lane * R + q] = (jl < nc && q < rc) ? x[(int64_t)(r0 + q) * ldx + dof] : V{};
                 }
+                __syncwarp();
                 const int jn = min(32, nc - j0);
-                const bool live = i0 < nr;  // lanes past the last row load nothing but still shuffle
                 const V *Bj = B + (int64_t)j0 * ld;
                 int jj = 0;
                 for (; jj + 8 <= jn; jj += 8) {
@@ -110,13 +124,14 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
                         }
                     }
 #pragma unroll
-                    for (int u = 0; u < 8; ++u)
+                    for (int u = 0; u < 8; ++u) {
+                        V xv[R];
+                        load_x<V, R>(xs + (jj + u) * R, xv);
 #pragma unroll
-                        for (int q = 0; q < R; ++q) {
-                            const V xv = shfl_idx(xr[q], jj + u);
+                        for (int q = 0; q < R; ++q)
 #pragma unroll
-                            for (int k = 0; k < RPL; ++k) acc[k][q] = fma_c(bv[u][k], xv, acc[k][q], cjg);
-                        }
+                            for (int k = 0; k < RPL; ++k) acc[k][q] = fma_c(bv[u][k], xv[q], acc[k][q], cjg);
+                    }
                 }
                 for (; jj < jn; ++jj) {
                     V bv[RPL];
@@ -128,7 +143,7 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
                     }
 #pragma unroll
                     for (int q = 0; q < R; ++q) {
-                        const V xv = shfl_idx(xr[q], jj);
+                        const V xv = xs[jj * R + q];
 #pragma unroll
                         for (int k = 0; k < RPL; ++k) acc[k][q] = fma_c(bv[k], xv, acc[k][q], cjg);
                     }
@@ -152,6 +167,115 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
         }
         __syncthreads();
     }
+}
+
+// Real near blocks with 8 or 16 right-hand sides on the FP64 tensor cores (mma.sync m8n8k4 f64).
+// A warp owns 64 rows (eight 8-row tiles) and all R = 8 * NT right-hand sides; per step of four
+// columns it loads its A fragments (the near block, one value per lane per row tile) straight
+// from HBM, its B fragments (x) from the warp's shared-memory chunk, and issues 8 * NT MMAs.
+// Fragment layout (PTX ISA, m8n8k4 .f64): A[lane/4][lane%4], B[lane%4][lane/4],
+// C[lane/4][2*(lane%4) + i]. Same block walk and reduction as near_rows_kernel.
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NEAR_WARPS * 32, 2)
+near_rows_mma_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const double *__restrict__ x,
+                     int64_t ldx, double *__restrict__ y, int64_t ldy, double alpha, double beta,
+                     bool beta_zero) {
+    constexpr int R = 8 * NT;
+    constexpr int XS = R + 4;  // padded row of the x chunk: conflict-free fragment reads
+    constexpr int RPP = 64;
+    extern __shared__ unsigned char smem_raw[];
+    const int g = blockIdx.x;
+    const int leaf = op.grp_leaf[g];
+    const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
+    const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g4 = lane >> 2, t4 = lane & 3;
+    double *xs = reinterpret_cast<double *>(smem_raw) + warp * 32 * XS;
+    double *part = reinterpret_cast<double *>(smem_raw) + NEAR_WARPS * 32 * XS;  // [NEAR_WARPS][RPP][R]
+    const double *D = static_cast<const double *>(op.data);
+    const int ld = nr + (nr & 1);
+    for (int p0 = 0; p0 < nr; p0 += RPP) {
+        double acc[8][NT][2];
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+#pragma unroll
+            for (int u = 0; u < NT; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
+        int unit = 0;
+        for (int bb = b0; bb < b1; ++bb) {
+            const int blk = op.grp_blk[bb];
+            const int inl = op.blk_in[blk];
+            const int c0 = ins.value_ptr[inl], nc = ins.value_ptr[inl + 1] - c0;
+            const double *B = D + op.blk_off[blk];
+            for (int j0 = 0; j0 < nc; j0 += 32, ++unit) {
+                if (unit % NEAR_WARPS != warp) continue;
+                __syncwarp();
+                {
+                    const int jl = j0 + lane;
+                    const int dof = jl < nc ? ins.value[c0 + jl] : 0;
+#pragma unroll
+                    for (int q = 0; q < R; ++q)
+                        xs[lane * XS + q] = (jl < nc && q < rc) ? x[(int64_t)(r0 + q) * ldx + dof] : 0.0;
+                }
+                __syncwarp();
+                const int jn = min(32, nc - j0);
+                for (int kk = 0; kk < jn; kk += 4) {
+                    const int col = kk + t4;
+                    const bool cv = col < jn;
+                    const double *bc = B + (int64_t)(j0 + col) * ld + p0 + g4;
+                    double a[8];
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) a[t] = (cv && p0 + 8 * t + g4 < nr) ? __ldcs(bc + 8 * t) : 0.0;
+                    double b[NT];
+#pragma unroll
+                    for (int u = 0; u < NT; ++u) b[u] = cv ? xs[col * XS + 8 * u + g4] : 0.0;
+#pragma unroll
+                    for (int t = 0; t < 8; ++t)
+#pragma unroll
+                        for (int u = 0; u < NT; ++u) dmma(acc[t][u], a[t], b[u]);
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+#pragma unroll
+            for (int u = 0; u < NT; ++u)
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+                    part[(warp * RPP + 8 * t + g4) * R + 8 * u + 2 * t4 + i] = acc[t][u][i];
+        __syncthreads();
+        const int rows = min(RPP, nr - p0);
+        for (int e = threadIdx.x; e < rows * rc; e += blockDim.x) {
+            const int i = e / rc, q = e % rc;
+            double sum = 0.0;
+#pragma unroll
+            for (int w = 0; w < NEAR_WARPS; ++w) sum += part[(w * RPP + i) * R + q];
+            double *o = &y[(int64_t)(r0 + q) * ldy + outs.value[o0 + p0 + i]];
+            const double v = alpha * sum;
+            *o = beta_zero ? v : v + beta * *o;
+        }
+        __syncthreads();
+    }
+}
+
+template <int NT>
+cudaError_t launch_rows_mma(const NearOp &op, const DSide &outs, const DSide &ins, int r0, int rc,
+                            const double *x, int64_t ldx, double *y, int64_t ldy, double alpha, double beta,
+                            bool bz, cudaStream_t st) {
+    constexpr int R = 8 * NT;
+    const size_t sm = (size_t)NEAR_WARPS * (32 * (R + 4) + 64 * R) * sizeof(double);
+    cudaError_t e = cudaSuccess;
+    if (sm > 48 * 1024)
+        e = cudaFuncSetAttribute(near_rows_mma_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    near_rows_mma_kernel<NT><<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, r0, rc, x, ldx, y, ldy,
+                                                                       alpha, beta, bz);
+    return cudaGetLastError();
 }
 
 // Build-time helpers --------------------------------------------------------------------------
@@ -211,7 +335,7 @@ cudaError_t launch_rows_t(const NearOp &op, const DSide &outs, const DSide &ins,
                           int rc, const V *x, int64_t ldx, V *y, int64_t ldy, V alpha, V beta,
                           bool bz, cudaStream_t st) {
     constexpr int RPP = 32 * NearVec<V>::RPL;
-    const size_t sm = (size_t)NEAR_WARPS * RPP * R * sizeof(V);
+    const size_t sm = (size_t)NEAR_WARPS * (32 + RPP) * R * sizeof(V);
     cudaError_t e = cudaSuccess;
     if (sm > 48 * 1024)
         e = cudaFuncSetAttribute(near_rows_kernel<V, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -229,6 +353,19 @@ cudaError_t near_apply_t(const NearOp &op, const DSide &outs, const DSide &ins, 
     for (int r0 = 0; r0 < nrhs; r0 += 16) {
         const int rc = std::min(16, nrhs - r0);
         cudaError_t e;
+        if constexpr (std::is_same<V, double>::value) {
+            // real blocks, 8 or more right-hand sides: FP64 tensor-core MMA
+            if (rc > 8) {
+                e = launch_rows_mma<2>(op, outs, ins, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+                if (e != cudaSuccess) return e;
+                continue;
+            }
+            if (rc == 8) {
+                e = launch_rows_mma<1>(op, outs, ins, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+                if (e != cudaSuccess) return e;
+                continue;
+            }
+        }
         if (rc == 1) e = launch_rows_t<V, 1>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
         else if (rc == 2) e = launch_rows_t<V, 2>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
         else if (rc <= 4) e = launch_rows_t<V, 4>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);

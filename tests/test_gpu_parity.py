@@ -146,7 +146,7 @@ def _x(core, nrhs, seed):
     return x[:, 0] if nrhs == 1 else x
 
 
-@pytest.mark.parametrize("nrhs", [1, 5])
+@pytest.mark.parametrize("nrhs", [1, 5, 8, 13])
 def test_methods_match_oracle(case, nrhs):
     name, core = case
     ws = h2.H2Workspace(core, max_nrhs=nrhs)
