@@ -378,6 +378,8 @@ def gpu_arm(args, rank, world, local_rank):
         wss.matvec_host(xpin, i % 2, y=ypin)
         te.append(time.perf_counter() - t1)
 
+    serving = serving_leg(torch, h2, core32, local_rank, args) if args.serve_seconds > 0 else None
+
     if rank != 0:
         return
     hbm, peak_kind = peaks()
@@ -416,7 +418,59 @@ def gpu_arm(args, rank, world, local_rank):
     }
     if cpu is not None:
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if serving is not None:
+        line["serving"] = serving
     print(json.dumps(line), flush=True)
+
+
+def serving_leg(torch, h2, core, local_rank, args):
+    """Closed-loop clients against the continuous-batching server on the served form's map.
+
+    Each client (an iterative solver) keeps one request in flight: forward / transpose / adjoint in
+    60 / 20 / 20 proportion on a device-resident vector, waits for the result, and submits the next.
+    Reports completed right-hand sides per second and per-request latency (submit to result).
+    """
+    from h2factory_b200.serving import GpuExecutor, MatvecServer
+
+    device = f"cuda:{local_rank}"
+    srv = MatvecServer(GpuExecutor(local_rank), budget_bytes=150e9, max_block=args.nrhs, slots=2)
+    srv.add_map("toeplitz", core)
+    n = core.trial.npoints
+    xs = [torch.randn(n, dtype=torch.float64, device=device) for _ in range(args.clients)]
+    torch.cuda.synchronize()
+    srv.submit("toeplitz", xs[0]).result(timeout=300)  # load the map and warm the slots
+    stop = [False]
+    counts = [0] * args.clients
+    t_start = [0.0]
+
+    def client(i):
+        r = np.random.default_rng(1000 + i)
+        while not stop[0]:
+            u = r.random()
+            mode = "forward" if u < 0.6 else ("transpose" if u < 0.8 else "adjoint")
+            srv.submit("toeplitz", xs[i], mode).result(timeout=300)
+            counts[i] += 1
+
+    ts = [threading.Thread(target=client, args=(i,), daemon=True) for i in range(args.clients)]
+    for t in ts:
+        t.start()
+    time.sleep(min(1.0, args.serve_seconds / 3))  # ramp up
+    base = sum(counts)
+    srv.latencies.clear()
+    srv.blocks.clear()
+    t0 = time.perf_counter()
+    time.sleep(args.serve_seconds)
+    done = sum(counts) - base
+    wall = time.perf_counter() - t0
+    stats = srv.stats()
+    stop[0] = True
+    for t in ts:
+        t.join(timeout=60)
+    srv.close()
+    return {"clients": args.clients, "mode_mix": "60/20/20 forward/transpose/adjoint",
+            "requests": done, "seconds": wall, "rhs_per_s": done / wall, "p50_ms": stats["p50_ms"],
+            "p99_ms": stats["p99_ms"], "mean_block": stats["mean_block"], "max_block": args.nrhs,
+            "requests_on_device": True}
 
 
 def core_with_host_near(core, near_host):
@@ -438,6 +492,8 @@ def main():
     ap.add_argument("--skip-check", action="store_true")
     ap.add_argument("--n", type=int, default=262144, help="points (smaller cases are for profiling)")
     ap.add_argument("--depth", type=int, default=5)
+    ap.add_argument("--clients", type=int, default=64, help="closed-loop clients of the serving leg")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving leg length (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
