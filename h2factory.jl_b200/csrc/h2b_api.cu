@@ -777,6 +777,15 @@ h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
     std::vector<int> ts;
     if (toep) ts = coupling_shapes(d);
     M.half_spectrum = toep && !cplx && couplings_hermitian(d, ts);
+    // specialised transforms when every level of both sides has (p, p, p) moments with 2p - 1 == 7
+    M.cube_ts = 0;
+    if (toep && d.dim == 3) {
+        bool cube = true;
+        for (const h2b_side_desc *sd : {&d.test, &d.trial})
+            for (int l = 1; l <= sd->nlevels; ++l)
+                cube &= sd->shape[3 * l] == 4 && sd->shape[3 * l + 1] == 4 && sd->shape[3 * l + 2] == 4;
+        if (cube) M.cube_ts = 7;
+    }
     h2b_status st = build_side(c, d, d.test, d.trial, c->test);
     if (st) return st;
     st = build_side(c, d, d.trial, d.test, c->trial);

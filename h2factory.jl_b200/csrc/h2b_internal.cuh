@@ -98,6 +98,7 @@ struct DMap {
     int ncomp, dim, nsectors;
     int transfer_kind, coupling_kind;
     int half_spectrum;       // Toeplitz spectra stored as half spectra (real maps, Hermitian couplings)
+    int cube_ts;             // > 0: every level's padded Toeplitz arrays are cube_ts^3 (3-D cubes)
     const int64_t *cpl_off;  // [ncouplings] offsets in elements of T (dense/diag) or spectrum (Toeplitz)
     const void *cpl;
 };

@@ -45,21 +45,23 @@ __device__ __forceinline__ int sep_bound(const DSide &s, int lp) {
 constexpr int TG_M = 64, TG_K = 32, TG_Q = 16, TG_LD = TG_K + 1;
 constexpr int TG_O = TG_M * TG_Q / 256;  // outputs per thread at 256 threads
 
-template <class T, class A, class XLoad>
-__device__ __forceinline__ void tile_gemm(const T *__restrict__ M, int64_t ldm, bool trans, bool cjg, int m0,
-                                          int mt, int kk, int nq, XLoad xload, A *Ms, A *Xs, A (&acc)[TG_O]) {
+// General form: mload(i, k) returns op(M)[i, k] in A; `kfast` says consecutive k are contiguous in
+// memory (so staging walks k fastest), otherwise consecutive i are.
+template <class A, class MLoad, class XLoad>
+__device__ __forceinline__ void tile_gemm_l(bool kfast, int m0, int mt, int kk, int nq, MLoad mload,
+                                            XLoad xload, A *Ms, A *Xs, A (&acc)[TG_O]) {
     for (int k0 = 0; k0 < kk; k0 += TG_K) {
         const int kc = min(TG_K, kk - k0);
         __syncthreads();
-        if (trans) {
+        if (kfast) {
             for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
                 const int k = idx % TG_K, i = idx / TG_K;
-                Ms[i * TG_LD + k] = k < kc ? wide(cj(M[(k0 + k) + (int64_t)(m0 + i) * ldm], cjg)) : A{};
+                Ms[i * TG_LD + k] = k < kc ? mload(m0 + i, k0 + k) : A{};
             }
         } else {
             for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
                 const int i = idx % mt, k = idx / mt;
-                Ms[i * TG_LD + k] = k < kc ? wide(cj(M[(m0 + i) + (int64_t)(k0 + k) * ldm], cjg)) : A{};
+                Ms[i * TG_LD + k] = k < kc ? mload(m0 + i, k0 + k) : A{};
             }
         }
         for (int idx = threadIdx.x; idx < TG_K * nq; idx += blockDim.x) {
@@ -79,6 +81,18 @@ __device__ __forceinline__ void tile_gemm(const T *__restrict__ M, int64_t ldm, 
             }
         }
     }
+}
+
+// op(M)[i, k] = M[i + k*ldm] (trans = false) or M[k + i*ldm] (trans = true), conjugated when cjg.
+template <class T, class A, class XLoad>
+__device__ __forceinline__ void tile_gemm(const T *__restrict__ M, int64_t ldm, bool trans, bool cjg, int m0,
+                                          int mt, int kk, int nq, XLoad xload, A *Ms, A *Xs, A (&acc)[TG_O]) {
+    if (trans)
+        tile_gemm_l(true, m0, mt, kk, nq, [&](int i, int k) -> A { return wide(cj(M[k + (int64_t)i * ldm], cjg)); },
+                    xload, Ms, Xs, acc);
+    else
+        tile_gemm_l(false, m0, mt, kk, nq, [&](int i, int k) -> A { return wide(cj(M[i + (int64_t)k * ldm], cjg)); },
+                    xload, Ms, Xs, acc);
 }
 
 template <class A>
@@ -191,6 +205,38 @@ __global__ void transfer_up_kernel(DMap m, DSide s, const int *__restrict__ node
     T *mp = am + s.mom_off[p] * nrhs;
     const int c0 = s.child_ptr[p], c1 = s.child_ptr[p + 1];
     const int nq = m.ncomp * nrhs;
+    if (m.transfer_kind == H2B_TRANSFER_DENSE && nq == 1) {
+        // one right-hand side: children split over `ns` thread groups of `npad` threads reading
+        // their transfers directly (coalesced over the output row), partial sums reduced in smem
+        const int npad = ((nout + 31) / 32) * 32;
+        const int ns = npad <= (int)blockDim.x ? (int)blockDim.x / npad : 1;
+        const int sidx = threadIdx.x / npad;
+        for (int a0 = 0; a0 < nout; a0 += (ns > 1 ? npad : (int)blockDim.x)) {
+            const int a = a0 + (ns > 1 ? (int)threadIdx.x % npad : (int)threadIdx.x);
+            A acc = sc_zero<A>();
+            if (sidx < ns && a < nout)
+                for (int k = c0 + sidx; k < c1; k += ns) {
+                    const int ch = s.child[k];
+                    const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
+                    const T *mc = am + s.mom_off[ch] * nrhs;
+#pragma unroll 4
+                    for (int b = 0; b < nin; ++b) acc = acc + wide(cj(Tk[a + (int64_t)b * nout], conjt)) * wide(mc[b]);
+                }
+            if (ns > 1) {
+                if (sidx < ns) sm[sidx * npad + (threadIdx.x % npad)] = acc;
+                __syncthreads();
+                if (threadIdx.x < npad && a0 + threadIdx.x < nout) {
+                    A sum = sm[threadIdx.x];
+                    for (int w = 1; w < ns; ++w) sum = sum + sm[w * npad + threadIdx.x];
+                    narrow(sum, mp[a0 + threadIdx.x]);
+                }
+                __syncthreads();
+            } else if (a < nout) {
+                narrow(acc, mp[a]);
+            }
+        }
+        return;
+    }
     if (m.transfer_kind == H2B_TRANSFER_DENSE) {
         A *Ms = sm, *Xs = sm + TG_M * TG_LD;
         for (int q0 = 0; q0 < nq; q0 += TG_Q) {
@@ -253,10 +299,13 @@ struct TGeom {
     int slen;    // stored spectrum length
 };
 
+// TS > 0: every level's moments are known to be (TS+1)/2-cubes, so the extents are compile-time
+// constants and the index arithmetic of the transforms folds to multiplications.
+template <int TS = 0>
 __device__ __forceinline__ TGeom tgeom(const DSide &s, int lvl, bool half) {
     TGeom g;
     for (int d = 0; d < 3; ++d) {
-        g.sh[d] = s.shape[3 * lvl + d];
+        g.sh[d] = TS > 0 ? (TS + 1) / 2 : s.shape[3 * lvl + d];
         g.ts[d] = 2 * g.sh[d] - 1;
     }
     g.nt = g.ts[0] * g.ts[1] * g.ts[2];
@@ -336,7 +385,7 @@ __device__ void dft_group(Cx<R> *a, const TGeom &g, bool inverse, Cx<R> *tw, int
 }
 
 // A3: spectrum(node) = F(pad(moment(node)))   (F = fft, or ifft for transpose maps)
-template <class T, int NMAX>
+template <class T, int NMAX, int TS>
 __global__ void __launch_bounds__(256) toeplitz_in_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
                                    int nrhs, int maxt, const T *__restrict__ am,
                                    typename ScalarTraits<T>::Complex *__restrict__ as) {
@@ -351,7 +400,7 @@ __global__ void __launch_bounds__(256) toeplitz_in_kernel(DMap m, DSide s, const
     const bool busy = t < ntrans;
     const int node = busy ? nodes[t / nq] : nodes[0];
     const int q = busy ? t % nq : 0;
-    const TGeom g = tgeom(s, s.level[node], m.half_spectrum != 0);
+    const TGeom g = tgeom<TS>(s, s.level[node], m.half_spectrum != 0);
     if (busy) {
         const T *mom = am + s.mom_off[node] * nrhs + (int64_t)q * g.nc;
         for (int e = tl; e < g.nt; e += FFT_T) {
@@ -373,7 +422,7 @@ __global__ void __launch_bounds__(256) toeplitz_in_kernel(DMap m, DSide s, const
 }
 
 // B3: moment(node) = corner(F^-1(spectrum(node)))   (overwrite)
-template <class T, int NMAX>
+template <class T, int NMAX, int TS>
 __global__ void __launch_bounds__(256) toeplitz_out_kernel(DMap m, DSide s, const int *__restrict__ nodes, int ntrans, bool inverse,
                                     int nrhs, int maxt,
                                     const typename ScalarTraits<T>::Complex *__restrict__ ds,
@@ -389,7 +438,7 @@ __global__ void __launch_bounds__(256) toeplitz_out_kernel(DMap m, DSide s, cons
     const bool busy = t < ntrans;
     const int node = busy ? nodes[t / nq] : nodes[0];
     const int q = busy ? t % nq : 0;
-    const TGeom g = tgeom(s, s.level[node], m.half_spectrum != 0);
+    const TGeom g = tgeom<TS>(s, s.level[node], m.half_spectrum != 0);
     if (busy) {
         const S *spec = ds + s.spec_off[node] * nrhs + (int64_t)q * g.slen;
         for (int e = tl; e < g.nt; e += FFT_T) {
@@ -437,7 +486,7 @@ __global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, cons
     if (m.coupling_kind == H2B_COUPLING_TOEPLITZ) {
         // each kernel value is loaded once and applied to up to QB right-hand sides
         constexpr int QB = 8;
-        const int nt = tgeom(r, lvl, m.half_spectrum != 0).slen;
+        const int nt = tgeom<>(r, lvl, m.half_spectrum != 0).slen;
         S *out = ds + r.spec_off[node] * nrhs;
         const S *K0 = static_cast<const S *>(m.cpl);
         for (int q0 = 0; q0 < nq; q0 += QB) {
@@ -770,6 +819,7 @@ cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DS
                                const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
                                int maxtsize, int maxaxis, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
+    const bool cube7 = m.cube_ts == 7;
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
@@ -786,7 +836,8 @@ cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DS
                     m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const T *>(fa.am), static_cast<S *>(fa.as));
             return e2;
         };
-        err = maxaxis <= 7 ? launch(toeplitz_in_kernel<T, 7>) : launch(toeplitz_in_kernel<T, 15>);
+        err = cube7 ? launch(toeplitz_in_kernel<T, 7, 7>)
+                    : (maxaxis <= 7 ? launch(toeplitz_in_kernel<T, 7, 0>) : launch(toeplitz_in_kernel<T, 15, 0>));
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
@@ -795,6 +846,7 @@ cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const D
                                 const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
                                 int maxtsize, int maxaxis, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
+    const bool cube7 = m.cube_ts == 7;
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
@@ -811,7 +863,8 @@ cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const D
                     m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const S *>(fa.ds), static_cast<T *>(fa.dm));
             return e2;
         };
-        err = maxaxis <= 7 ? launch(toeplitz_out_kernel<T, 7>) : launch(toeplitz_out_kernel<T, 15>);
+        err = cube7 ? launch(toeplitz_out_kernel<T, 7, 7>)
+                    : (maxaxis <= 7 ? launch(toeplitz_out_kernel<T, 7, 0>) : launch(toeplitz_out_kernel<T, 15, 0>));
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
@@ -843,6 +896,8 @@ cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const D
     const int bs = block_for(maxslen, 32, 512);
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
+        // two right-hand sides per CTA share each kernel value load (one-wide blocks reload them
+        // per right-hand side, which costs more than the lower occupancy of the wider block)
         if (nq == 1)
             i2o_sibling_kernel<T, 1><<<dim3(g.ngroups, 1), bs, 0, st>>>(
                 m, recv, g, fa.mode, fa.nrhs, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
