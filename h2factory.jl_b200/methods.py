@@ -115,9 +115,12 @@ def _node_grid(tree: Tree, n: int, nodes: np.ndarray) -> np.ndarray:
 def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
                        transfers: str = "dense", couplings: str = "dense",
                        field: str | None = None, precision: str = "fp64",
-                       near: str = "host", alpha=1.0) -> H2Core:
-    """Galerkin H2 core of an interpolation FMM of order `p` on `tree` for `kernel`.
+                       near: str = "host", alpha=1.0, trial: Tree | None = None) -> H2Core:
+    """H2 core of an interpolation FMM of order `p` for `kernel`.
 
+    `tree` holds the test (row) points; `trial` the trial (column) points of a Petrov map
+    (test/farinteractions/test_rectangular.jl), or None for a Galerkin map on one tree. The two
+    trees must share the root box so that their boxes pair level by level.
     couplings = "dense" stores one M2L block per unique translation; "toeplitz" stores the
     FFT'd wrap-around kernel per unique translation (equispaced nodes, same-size boxes only).
     near = "host" assembles near blocks on the host; "none" leaves them to the caller
@@ -126,22 +129,32 @@ def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
     xi = chebyshev_nodes(p) if nodes == "chebyshev" else equispaced_nodes(p)
     if couplings == "toeplitz" and nodes != "equispaced":
         raise ValueError("Toeplitz couplings need equispaced interpolation nodes")
-    plans = build_plans(tree)
+    test = tree
+    trial = tree if trial is None else trial
+    if trial is not test and (not np.allclose(test.center[0], trial.center[0])
+                              or not np.isclose(test.halfsize[0], trial.halfsize[0])):
+        raise ValueError("test and trial trees need the same root box")
+    plans = build_plans(test, trial)
     dim = tree.dim
     cplx = np.iscomplexobj(kernel(np.zeros((1, dim)), np.ones((1, dim))))
     if field is None:
         field = "complex" if cplx else "real"
     dtype = np.complex128 if field == "complex" else np.float64
-    shape = np.zeros((tree.nlevels + 1, 3), np.int32)
-    shape[1:, :] = 1
-    shape[1:, :dim] = p
+    def side_shape(t):
+        sh = np.zeros((t.nlevels + 1, 3), np.int32)
+        sh[1:, :] = 1
+        sh[1:, :dim] = p
+        return sh
 
-    leaves = tree.leaves()
-    colls = {int(n): _leaf_collection(tree, int(n), xi).astype(dtype)[None] for n in leaves}
+    def side_colls(t):
+        return {int(n): _leaf_collection(t, int(n), xi).astype(dtype)[None] for n in t.leaves()}
+
+    colls = side_colls(test)
+    colls_trial = colls if trial is test else side_colls(trial)
 
     lo, hi = _axis_factors(xi)
     tdict = {}
-    for lvl in range(2, tree.nlevels + 1):
+    for lvl in range(2, max(test.nlevels, trial.nlevels) + 1):
         for s in range(tree.nsectors):
             facs = [(hi if (s >> d) & 1 else lo).astype(dtype) for d in range(dim)]
             if transfers == "separable":
@@ -153,20 +166,20 @@ def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
                 tdict[(lvl, s)] = T
 
     far = plans.far
-    ca, cb = tree.center[far[:, 0]], tree.center[far[:, 1]]
-    hmin = np.minimum(tree.halfsize[far[:, 0]], tree.halfsize[far[:, 1]])
+    ca, cb = test.center[far[:, 0]], trial.center[far[:, 1]]
+    hmin = np.minimum(test.halfsize[far[:, 0]], trial.halfsize[far[:, 1]])
     offs = np.round((cb - ca) / hmin[:, None] * 2).astype(np.int64)
-    keys = np.concatenate([tree.level[far[:, 0]][:, None].astype(np.int64),
-                           tree.level[far[:, 1]][:, None].astype(np.int64), offs], axis=1)
+    keys = np.concatenate([test.level[far[:, 0]][:, None].astype(np.int64),
+                           trial.level[far[:, 1]][:, None].astype(np.int64), offs], axis=1)
     ukeys, first, inv = np.unique(keys, axis=0, return_index=True, return_inverse=True)
     blocks = []
     for u in range(ukeys.shape[0]):
         r, t = int(far[first[u], 0]), int(far[first[u], 1])
         if couplings == "toeplitz":
-            if tree.level[r] != tree.level[t]:
+            if test.level[r] != trial.level[t]:
                 raise ValueError("Toeplitz couplings need same-level pairs (uniform trees)")
-            h = tree.halfsize[r]
-            dc = tree.center[r] - tree.center[t]
+            h = test.halfsize[r]
+            dc = test.center[r] - trial.center[t]
             ts = 2 * p - 1
             m = np.arange(ts)
             m = np.where(m < p, m, m - ts)          # wrap-around: index mod(i - j, ts)
@@ -175,18 +188,18 @@ def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
             kv = kernel(z.reshape(-1, dim), np.zeros((1, dim)))[:, 0].reshape((ts,) * dim)
             blocks.append(np.fft.fftn(kv.astype(np.complex128)))
         else:
-            B = kernel(_node_grid(tree, r, xi), _node_grid(tree, t, xi)).astype(dtype)
+            B = kernel(_node_grid(test, r, xi), _node_grid(trial, t, xi)).astype(dtype)
             blocks.append(B)
 
-    core = H2Core(field=field, test=tree, trial=tree, plans=plans, ncomp=1, dim=dim,
-                  shape_test=shape, shape_trial=shape, collections_test=colls,
-                  collections_trial=colls, transfers_test=tdict, transfers_trial=tdict,
+    core = H2Core(field=field, test=test, trial=trial, plans=plans, ncomp=1, dim=dim,
+                  shape_test=side_shape(test), shape_trial=side_shape(trial), collections_test=colls,
+                  collections_trial=colls_trial, transfers_test=tdict, transfers_trial=tdict,
                   transfer_kind=transfers, coupling_kind=couplings, couplings=blocks,
                   pair_coupling=inv.reshape(-1).astype(np.int64), precision=precision,
                   alpha=alpha, conj_leaf_adjoint=(field == "complex"))
     core.kernel = kernel
     if near == "host":
-        core.set_near_blocks(near_blocks_from_kernel(tree, plans, kernel, dtype))
+        core.set_near_blocks(near_blocks_from_kernel(trial, plans, kernel, dtype, test=test))
     return core
 
 

@@ -104,3 +104,71 @@ def manyclusters(k, n, gap=100.0, spread=0.1):
             pts.append((c * gap + spread * j / (n - 1), 0.0, 0.0))
             cid.append(c)
     return np.array(pts), np.array(cid)
+
+
+def petrov_core(ntest=256, ntrial=16, c_trial=2.0, c_test=3.0, c_i2o=0.75 - 1.25j):
+    """Rectangular Petrov map with side-owned scalar transfers.
+
+    Restates test/farinteractions/test_rectangular.jl:44-76: uniform points on [0, 1] on each
+    side (different counts, hence different tree depths), leaf bases of ones, every trial-side
+    I2I/O2O equal to c_trial, every test-side one equal to c_test (real, so that the transposed
+    and adjoint factors stay exact), and one complex coupling c_i2o. The complete matrix is
+    F[i, j] = sum over far pairs (a, b) with i under a and j under b of
+    c_test^(level(leaf(i)) - level(a)) * c_i2o * c_trial^(level(leaf(j)) - level(b)),
+    assembled here from the trees alone. Near blocks hold 1 / (1 + |s - t|).
+    """
+    def side(n):
+        pts = ((np.arange(n) + 0.5) / n)[:, None]
+        return build_tree(pts, maxvalues=1, minhalfsize=0.004, root_center=[0.5], root_halfsize=0.5)
+
+    test, trial = side(ntest), side(ntrial)
+    plans = build_plans(test, trial)
+
+    def shape(t):
+        sh = np.zeros((t.nlevels + 1, 3), np.int32)
+        sh[1:] = (1, 1, 1)
+        return sh
+
+    def colls(t):
+        return {int(l): np.ones((1, 1, t.values(int(l)).size), np.complex128) for l in t.leaves()}
+
+    def transfers(t, c):
+        return {(l, s): np.full((1, 1), c, np.complex128) for l in range(2, t.nlevels + 1)
+                for s in range(t.nsectors)}
+
+    core = H2Core(field="complex", test=test, trial=trial, plans=plans, ncomp=1, dim=1,
+                  shape_test=shape(test), shape_trial=shape(trial), collections_test=colls(test),
+                  collections_trial=colls(trial), transfers_test=transfers(test, c_test),
+                  transfers_trial=transfers(trial, c_trial), transfer_kind="dense",
+                  coupling_kind="dense", couplings=[np.array([[c_i2o]], np.complex128)],
+                  pair_coupling=np.zeros(plans.far.shape[0], np.int64), alpha=1.0,
+                  conj_leaf_adjoint=True)
+
+    def chains(t):
+        """Per point: its leaf's level and its ancestor at every level (-1 below the leaf)."""
+        anc = np.full((t.npoints, t.nlevels + 1), -1, np.int64)
+        lvl = np.zeros(t.npoints, np.int64)
+        for leaf in t.leaves():
+            v = t.values(int(leaf))
+            lvl[v] = t.level[leaf]
+            n = int(leaf)
+            while n >= 0:
+                anc[v, t.level[n]] = n
+                n = int(t.parent[n])
+        return anc, lvl
+
+    (ai, li), (aj, lj) = chains(test), chains(trial)
+    F = np.zeros((ntest, ntrial), np.complex128)
+    for a, b in plans.far:
+        rows = np.nonzero(ai[:, test.level[a]] == a)[0]
+        cols = np.nonzero(aj[:, trial.level[b]] == b)[0]
+        F[np.ix_(rows, cols)] += (np.power(c_test, li[rows] - test.level[a])[:, None] * c_i2o
+                                  * np.power(c_trial, lj[cols] - trial.level[b])[None, :])
+    blocks, N = [], np.zeros_like(F)
+    for a, b in plans.near:
+        va, vb = test.values(int(a)), trial.values(int(b))
+        blk = 1.0 / (1.0 + np.abs(test.points[va, 0][:, None] - trial.points[vb, 0][None, :]))
+        blocks.append(blk.astype(np.complex128))
+        N[np.ix_(va, vb)] = blk
+    core.set_near_blocks(blocks)
+    return core, F, N

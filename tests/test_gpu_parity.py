@@ -122,6 +122,12 @@ CASES = {
     # so the per-node Toeplitz kernel runs
     "toeplitz-laplace-unshared": lambda: _unshared(methods.interpolation_core(
         _cube(2000, 5, depth=3), methods.laplace, 4, nodes="equispaced", couplings="toeplitz")),
+    # Petrov (rectangular) maps: test and trial trees on different point sets and depths
+    "petrov-cheb-laplace": lambda: methods.interpolation_core(
+        _cube(3000, 6, maxvalues=40), methods.laplace, 4, trial=_cube(1100, 7, maxvalues=30)),
+    "petrov-toeplitz-helmholtz": lambda: methods.interpolation_core(
+        _cube(2500, 8, depth=4), methods.helmholtz(3.0), 3, nodes="equispaced", couplings="toeplitz",
+        trial=_cube(4000, 9, depth=4)),
 }
 
 
@@ -137,9 +143,10 @@ def case(request):
     return request.param, core
 
 
-def _x(core, nrhs, seed):
+def _x(core, nrhs, seed, mode=0, out=False):
+    """Right-hand sides of op(A) (out=False) or its outputs (out=True) for orientation `mode`."""
     rng = np.random.default_rng(seed)
-    n = core.trial.npoints
+    n = core.trial.npoints if (mode == 0) != out else core.test.npoints
     x = rng.standard_normal((n, nrhs))
     if core.field == "complex":
         x = x + 1j * rng.standard_normal((n, nrhs))
@@ -150,9 +157,9 @@ def _x(core, nrhs, seed):
 def test_methods_match_oracle(case, nrhs):
     name, core = case
     ws = h2.H2Workspace(core, max_nrhs=nrhs)
-    x = _x(core, nrhs, 11)
     desc = h2.flatten(core)
     for mode, op in ORIENT:
+        x = _x(core, nrhs, 11, mode)
         want = oracle.matvec(core, x, mode, desc=desc)
         got = run(h2.mul_, op(ws), x)
         assert rel(got, want) < TOL64, (name, mode)
@@ -161,11 +168,11 @@ def test_methods_match_oracle(case, nrhs):
 def test_methods_scaled_and_partial_products(case):
     name, core = case
     ws = h2.H2Workspace(core, max_nrhs=3)
-    x = _x(core, 3, 12)
-    y0 = _x(core, 3, 13)
     a, b = (0.75 - 0.5j, -1.25 + 0.3j) if core.field == "complex" else (0.75, -1.25)
     desc = h2.flatten(core)
     for mode, op in ORIENT:
+        x = _x(core, 3, 12, mode)
+        y0 = _x(core, 3, 13, mode, out=True)
         want = oracle.matvec(core, x, mode, alpha=a, beta=b, y=y0, desc=desc)
         assert rel(run(h2.mul_, op(ws), x, y0=y0, alpha=a, beta=b), want) < TOL64, (name, mode)
         want = oracle.farmul(core, x, mode, desc=desc)
@@ -178,10 +185,10 @@ def test_methods_scaled_and_partial_products(case):
 
 def test_fp32_far_field_form(case):
     name, core = case
-    x = _x(core, 5, 14)
     core32 = methods_copy_fp32(core)
     ws = h2.H2Workspace(core32, max_nrhs=5)
     for mode, op in ORIENT:
+        x = _x(core, 5, 14, mode)
         want = oracle.matvec(core, x, mode)
         assert rel(run(h2.mul_, op(ws), x), want) < TOL32, (name, mode)
 
@@ -198,8 +205,8 @@ def test_host_buffer_path(case):
     """h2b_matvec_host: host arrays in and out, the call a host-language binding makes."""
     name, core = case
     ws = h2.H2Workspace(core, max_nrhs=2)
-    x = _x(core, 2, 15)
     for mode in (0, 1, 2):
+        x = _x(core, 2, 15, mode)
         got = ws.matvec_host(x, mode)
         assert rel(got, oracle.matvec(core, x, mode)) < TOL64, (name, mode)
 
@@ -213,6 +220,24 @@ def test_two_workspaces_share_one_core():
     ya = run(h2.mul_, a, x)
     yb = run(h2.mul_, b, x)
     assert rel(ya, yb) == 0.0
+
+
+@pytest.mark.parametrize("ntest,ntrial", [(256, 16), (16, 256)])
+def test_petrov_side_owned_transfers_gpu(ntest, ntrial):
+    """test/farinteractions/test_rectangular.jl:103-154 on the device: all orientations equal the
+    complete matrix of a rectangular map with distinct per-side transfers."""
+    from fakes import petrov_core
+
+    core, F, N = petrov_core(ntest, ntrial)
+    ws = h2.H2Workspace(core, max_nrhs=2)
+    rng = np.random.default_rng(20260720)
+    x = rng.standard_normal((ntrial, 2)) + 1j * rng.standard_normal((ntrial, 2))
+    y = rng.standard_normal((ntest, 2)) + 1j * rng.standard_normal((ntest, 2))
+    assert rel(run(h2.farmul_, ws, x), F @ x) < TOL64
+    assert rel(run(h2.farmul_, h2.transpose(ws), y), F.T @ y) < TOL64
+    assert rel(run(h2.farmul_, h2.adjoint(ws), y), F.conj().T @ y) < TOL64
+    assert rel(run(h2.mul_, ws, x), (F + N) @ x) < TOL64
+    assert rel(run(h2.mul_, h2.adjoint(ws), y), (F + N).conj().T @ y) < TOL64
 
 
 def test_single_leaf_map_has_no_far_field():

@@ -135,3 +135,18 @@ def test_scaled_mul_and_farmul_rules(cube_tree):
         near = oracle.nearmul(core, x, mode)
         far = oracle.farmul(core, x, mode)
         assert rel(near + far, full) < 1e-13
+
+
+def test_petrov_interpolation_vs_dense():
+    """Rectangular map (test points != trial points, different depths) against the dense kernel
+    in all orientations: the traversal pairs boxes of two trees on one root box."""
+    rng = np.random.default_rng(6)
+    test = build_tree(rng.random((3000, 3)), maxvalues=20, root_center=[0.5] * 3, root_halfsize=0.5)
+    trial = build_tree(rng.random((300, 3)), maxvalues=40, root_center=[0.5] * 3, root_halfsize=0.5)
+    core = methods.interpolation_core(test, methods.helmholtz(2.0), 4, trial=trial)
+    assert core.test.nlevels != core.trial.nlevels
+    K = methods.kernel_matrix(core.kernel, test.points, trial.points)
+    for mode, op in ((0, K), (1, K.T), (2, K.conj().T)):
+        x = rng.standard_normal(op.shape[1]) + 1j * rng.standard_normal(op.shape[1])
+        y = oracle.matvec(core, x, mode)
+        assert np.linalg.norm(y - op @ x) / np.linalg.norm(op @ x) < 5e-3
