@@ -179,6 +179,19 @@ def time_loop(torch, fn, steps, warmup, stream):
     return per, ev[0].elapsed_time(ev[steps])
 
 
+def max_over_ranks(torch, values, world, device):
+    """Each value's maximum over the replicas (the job time is the slowest rank's)."""
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_rate(units_per_rank, world, total_ms):
+    """Whole-job throughput of `world` replicas that each processed `units_per_rank` units."""
+    return units_per_rank * world / (total_ms * 1e-3)
+
+
 def pct(v, q):
     return float(np.percentile(np.asarray(v), q))
 
@@ -362,10 +375,7 @@ def gpu_arm(args, rank, world, local_rank):
         xn = xp[:, 0].contiguous()
         nper, ntotal = time_loop(torch, lambda i: h2.nearmul_(yn, wsp, xn, stream=sptr),
                                  max(args.steps, 5), 3, torch.cuda.current_stream(device))
-    times = torch.tensor([tot_p, tot_s], dtype=torch.float64, device=device)
-    if world > 1:
-        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
-    tot_p, tot_s = float(times[0]), float(times[1])
+    tot_p, tot_s = max_over_ranks(torch, [tot_p, tot_s], world, device)
 
     # end to end through the host-buffer C-ABI call (pinned host memory, copies inside the region)
     xpin = torch.from_numpy(np.asfortranarray(xhs)).pin_memory().numpy()
@@ -380,6 +390,24 @@ def gpu_arm(args, rank, world, local_rank):
 
     serving = serving_leg(torch, h2, core32, local_rank, args) if args.serve_seconds > 0 else None
 
+    # the same map with a matrix-free near field (entries recomputed from the points, no stored
+    # blocks): its own form, reported beside the stored-block forms
+    mf = None
+    if args.matrix_free:
+        free = copy.copy(core)
+        free.set_near_kernel("laplace")
+        free32 = copy.copy(free)
+        free32.precision = "fp32"
+        steps_mf = max(3, args.steps // 10)
+        wfp, _, _, _, tfp = form_run(torch, h2, free, 1, steps_mf, args.warmup, device, 7 + rank)
+        wfs, _, _, _, tfs = form_run(torch, h2, free32, nserve, steps_mf, args.warmup, device, 11 + rank)
+        tfp, tfs = max_over_ranks(torch, [tfp, tfs], world, device)
+        mf = {"plain_rhs_per_s": job_rate(steps_mf, world, tfp), "served_rhs_per_s": job_rate(steps_mf * nserve, world, tfs),
+              "steps": steps_mf, "near_bytes_stored": 0, "device_bytes": int(wfp.dcore.info().device_bytes)}
+        for w in (wfp, wfs):
+            w.close()
+            w.dcore.close()
+
     if rank != 0:
         return
     hbm, peak_kind = peaks()
@@ -390,8 +418,8 @@ def gpu_arm(args, rank, world, local_rank):
     workload = WORKLOAD if (args.n, args.depth) == (262144, 5) else f"toeplitz-laplace-N{args.n}-depth{args.depth}-p4"
     traffic = traffic_table().get(("near_rows_kernel", workload))
     launches = (sum(launches_per_step(core, i % 2) for i in range(args.steps)) * 2)
-    plain_rate = args.steps * world / (tot_p * 1e-3)
-    served_rate = args.steps * nserve * world / (tot_s * 1e-3)
+    plain_rate = job_rate(args.steps, world, tot_p)
+    served_rate = job_rate(args.steps * nserve, world, tot_s)
     line = {
         "metric": METRIC, "value": served_rate, "unit": "RHS/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_s / args.steps,
@@ -416,6 +444,8 @@ def gpu_arm(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "gpu_launches": launches,
     }
+    if mf is not None:
+        line["matrix_free_near"] = mf
     if cpu is not None:
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if serving is not None:
@@ -494,6 +524,8 @@ def main():
     ap.add_argument("--depth", type=int, default=5)
     ap.add_argument("--clients", type=int, default=64, help="closed-loop clients of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving leg length (0: skip)")
+    ap.add_argument("--no-matrix-free", dest="matrix_free", action="store_false",
+                    help="skip the matrix-free near-field forms")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))

@@ -53,6 +53,10 @@ class MapDesc(C.Structure):
         ("near_nrows", C.c_int32), ("near_row", _i32p), ("near_ptr", _i32p), ("near_col", _i32p),
         ("near_offset", _i64p), ("near", _f64p), ("near_len", C.c_int64),
         ("near_on_device", C.c_int32),
+        ("near_kind", C.c_int32), ("near_wavenumber", C.c_double), ("test_points", _f64p),
+        ("trial_points", _f64p),
+        ("coupling_rowperm", _i64p), ("coupling_colperm", _i64p), ("coupling_perm", _i32p),
+        ("coupling_perm_len", C.c_int64),
     ]
 
 
@@ -75,6 +79,8 @@ EXPORTS = [
 ]
 
 H2B_NOALLOC_SCRATCH_BYTES = 16 << 20
+
+H2B_NEAR_STORED, H2B_NEAR_LAPLACE, H2B_NEAR_HELMHOLTZ = 0, 1, 2
 
 
 class H2BError(RuntimeError):

@@ -56,6 +56,13 @@ class H2Core:
     near_offset: np.ndarray | None = None
     near_device: object = None      # torch tensor holding near blocks on the device
     kernel: object = field(default=None, repr=False)
+    near_kind: str = "stored"       # "stored" blocks, or a point kernel: "laplace" | "helmholtz"
+    near_wavenumber: float = 0.0    # k of the Helmholtz point kernel
+    # symmetry-reduced couplings: `couplings` holds one canonical block per orbit; key k (the
+    # values of pair_coupling) reads couplings[coupling_canon[k]] through its permutations
+    coupling_canon: np.ndarray | None = None
+    coupling_rowperm: list | None = None  # per key: int32 array or None (identity)
+    coupling_colperm: list | None = None  # per key (dense only)
 
     @property
     def dtype(self):
@@ -87,6 +94,19 @@ class H2Core:
         self.near_device = tensor
         self.near_offset = np.asarray(offsets, np.int64)
         self.near_data = None
+
+    def set_near_kernel(self, kind: str, wavenumber: float = 0.0):
+        """Matrix-free near field: entries K(x_i, y_j) computed on the device from the points.
+
+        A custom near storage in the sense of docs/src/near/storage.md:7-14 (any matrix-like
+        operator with `mul!`): "laplace" is 1/(4 pi r), "helmholtz" exp(i k r)/(4 pi r), both 0 at
+        r = 0 -- the kernels of h2factory_b200.methods -- over the same near leaf pairs.
+        """
+        if kind not in ("laplace", "helmholtz"):
+            raise ValueError(kind)
+        self.near_kind = kind
+        self.near_wavenumber = float(wavenumber)
+        self.near_data = self.near_offset = self.near_device = None
 
     def near_block(self, k: int) -> np.ndarray:
         a, b = self.plans.near[k]
@@ -204,10 +224,37 @@ def flatten(core: H2Core):
         coffs.append(pos)
         parts.append(flat)
         pos += flat.size
-    d.ncouplings = len(coffs)
-    d.coupling_offset = keep.add(np.array(coffs if coffs else [0], np.int64), C.c_int64)
     d.coupling = keep.add(np.concatenate(parts) if parts else np.zeros(1), C.c_double)
     d.coupling_len = pos
+    if core.coupling_canon is None:
+        d.ncouplings = len(coffs)
+        d.coupling_offset = keep.add(np.array(coffs if coffs else [0], np.int64), C.c_int64)
+    else:
+        # one key per translation, sharing its orbit's canonical data, plus its permutations
+        canon = np.asarray(core.coupling_canon, np.int64)
+        d.ncouplings = canon.size
+        d.coupling_offset = keep.add(np.array(coffs, np.int64)[canon] if canon.size else np.zeros(1, np.int64),
+                                     C.c_int64)
+        store, chunks, at = {}, [], 0
+
+        def perm_offset(pm):
+            nonlocal at
+            if pm is None:
+                return -1
+            pm = np.ascontiguousarray(pm, np.int32)
+            key = pm.tobytes()
+            if key not in store:
+                store[key] = at
+                chunks.append(pm)
+                at += pm.size
+            return store[key]
+
+        rows = np.array([perm_offset(pm) for pm in core.coupling_rowperm], np.int64)
+        cols = np.array([perm_offset(pm) for pm in (core.coupling_colperm or [None] * canon.size)], np.int64)
+        d.coupling_rowperm = keep.add(rows if rows.size else np.full(1, -1, np.int64), C.c_int64)
+        d.coupling_colperm = keep.add(cols if cols.size else np.full(1, -1, np.int64), C.c_int64)
+        d.coupling_perm = keep.add(np.concatenate(chunks) if chunks else np.zeros(1, np.int32), C.c_int32)
+        d.coupling_perm_len = at
 
     near = core.plans.near
     rows, starts = np.unique(near[:, 0], return_index=True) if near.size else (np.zeros(0, np.int32), np.zeros(0, np.int64))
@@ -229,6 +276,14 @@ def flatten(core: H2Core):
         d.near = keep.add(_as_f64(data), C.c_double)
         d.near_len = data.size if core.near_data is not None else 0
         d.near_on_device = 0
+    d.near_kind = {"stored": _abi.H2B_NEAR_STORED, "laplace": _abi.H2B_NEAR_LAPLACE,
+                   "helmholtz": _abi.H2B_NEAR_HELMHOLTZ}[core.near_kind]
+    d.near_wavenumber = core.near_wavenumber
+    if core.near_kind != "stored":
+        for name, tree in (("test_points", core.test), ("trial_points", core.trial)):
+            pts = np.zeros((tree.npoints, 3))
+            pts[:, :tree.dim] = tree.points
+            setattr(d, name, keep.add(pts, C.c_double))
     return d, keep
 
 

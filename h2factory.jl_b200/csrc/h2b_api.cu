@@ -14,6 +14,7 @@
 #include <map>
 #include <new>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "h2b_internal.cuh"
@@ -156,7 +157,7 @@ int64_t spec_len(const h2b_side_desc &s, int lvl, bool half) {
 }
 
 h2b_status validate_side(const h2b_map_desc &d, const h2b_side_desc &s, const h2b_side_desc &other,
-                         const char *name) {
+                         const char *name, std::vector<int64_t> &permlen) {
     if (s.nnodes < 1 || s.nlevels < 1 || s.ndofs < 0)
         return fail(H2B_ERR_INVALID, "%s: nnodes/nlevels must be positive", name);
     if (!s.level || !s.parent || !s.sector || !s.child_ptr || !s.value_ptr || !s.shape ||
@@ -278,6 +279,22 @@ h2b_status validate_side(const h2b_map_desc &d, const h2b_side_desc &s, const h2
             }
             if (off < 0 || off + need > d.coupling_len)
                 return fail(H2B_ERR_INVALID, "%s: coupling %lld exceeds the coupling array", name, (long long)key);
+            if (d.coupling_rowperm) {
+                // permuted couplings: square dense blocks (one grid permutation per side) or
+                // Toeplitz tensors; the length each permutation must have
+                int64_t len;
+                if (d.coupling_kind == H2B_COUPLING_DENSE) {
+                    if (nr != nt) return fail(H2B_ERR_INVALID, "%s: permuted coupling between different sizes", name);
+                    len = nr;
+                } else if (d.coupling_kind == H2B_COUPLING_TOEPLITZ) {
+                    len = tsize_host(s, s.level[n]);
+                } else {
+                    return fail(H2B_ERR_UNSUPPORTED, "permuted diagonal couplings");
+                }
+                if (permlen[key] >= 0 && permlen[key] != len)
+                    return fail(H2B_ERR_INVALID, "%s: coupling %lld used with two sizes", name, (long long)key);
+                permlen[key] = len;
+            }
         }
     // leaf collections of every leaf either plan touches
     const int fw = d.field == H2B_COMPLEX ? 2 : 1;
@@ -332,10 +349,35 @@ h2b_status validate(const h2b_map_desc &d) {
     }
     if (d.coupling_len < 0 || (d.coupling_len > 0 && !d.coupling)) return fail(H2B_ERR_INVALID, "coupling array missing");
     if (d.near_len < 0 || (d.near_len > 0 && !d.near)) return fail(H2B_ERR_INVALID, "near array missing");
-    h2b_status st = validate_side(d, d.test, d.trial, "test");
+    std::vector<int64_t> permlen(std::max<int64_t>(d.ncouplings, 1), -1);
+    if (d.coupling_rowperm && (!d.coupling_perm || d.coupling_perm_len < 0 ||
+                               (d.coupling_kind == H2B_COUPLING_DENSE && !d.coupling_colperm)))
+        return fail(H2B_ERR_INVALID, "coupling permutation arrays");
+    h2b_status st = validate_side(d, d.test, d.trial, "test", permlen);
     if (st) return st;
-    st = validate_side(d, d.trial, d.test, "trial");
+    st = validate_side(d, d.trial, d.test, "trial", permlen);
     if (st) return st;
+    if (d.coupling_rowperm) {
+        // every permutation within the array and a permutation of 0 .. len-1
+        std::vector<int> seen;
+        for (int64_t k = 0; k < d.ncouplings; ++k) {
+            if (permlen[k] < 0) continue;
+            for (int w = 0; w < 2; ++w) {
+                const int64_t *po = w == 0 ? d.coupling_rowperm : d.coupling_colperm;
+                if (!po || (w == 1 && d.coupling_kind != H2B_COUPLING_DENSE)) continue;
+                const int64_t o = po[k];
+                if (o < -1 || (o >= 0 && o + permlen[k] > d.coupling_perm_len))
+                    return fail(H2B_ERR_INVALID, "coupling %lld: permutation out of range", (long long)k);
+                if (o < 0) continue;
+                seen.assign(permlen[k], 0);
+                for (int64_t i = 0; i < permlen[k]; ++i) {
+                    const int v = d.coupling_perm[o + i];
+                    if (v < 0 || v >= permlen[k] || seen[v]++)
+                        return fail(H2B_ERR_INVALID, "coupling %lld: not a permutation", (long long)k);
+                }
+            }
+        }
+    }
     if (d.coupling_kind == H2B_COUPLING_TOEPLITZ) {
         for (const h2b_side_desc *s : {&d.test, &d.trial})
             for (int l = 1; l <= s->nlevels; ++l)
@@ -344,8 +386,16 @@ h2b_status validate(const h2b_map_desc &d) {
                         return fail(H2B_ERR_UNSUPPORTED, "Toeplitz moments are limited to 8 points per axis");
     }
     // near blocks
+    const bool stored = d.near_kind == H2B_NEAR_STORED;
+    if (d.near_kind < H2B_NEAR_STORED || d.near_kind > H2B_NEAR_HELMHOLTZ)
+        return fail(H2B_ERR_INVALID, "unknown near kind %d", d.near_kind);
+    if (!stored && (!d.test_points || !d.trial_points))
+        return fail(H2B_ERR_INVALID, "matrix-free near field without points");
+    if (d.near_kind == H2B_NEAR_HELMHOLTZ && d.field != H2B_COMPLEX)
+        return fail(H2B_ERR_INVALID, "Helmholtz near kernel on a real map");
+    if (!stored && !std::isfinite(d.near_wavenumber)) return fail(H2B_ERR_INVALID, "near wavenumber");
     if (d.near_nrows < 0) return fail(H2B_ERR_INVALID, "near_nrows");
-    if (d.near_nrows > 0 && (!d.near_row || !d.near_ptr || !d.near_offset || !d.near))
+    if (d.near_nrows > 0 && (!d.near_row || !d.near_ptr || (stored && (!d.near_offset || !d.near))))
         return fail(H2B_ERR_INVALID, "near arrays");
     if (d.near_nrows > 0 && d.near_ptr[0] != 0) return fail(H2B_ERR_INVALID, "near_ptr[0] != 0");
     for (int g = 0; g < d.near_nrows; ++g) {
@@ -359,7 +409,7 @@ h2b_status validate(const h2b_map_desc &d) {
             if (col < 0 || col >= d.trial.nnodes || !isleaf(d.trial, col))
                 return fail(H2B_ERR_INVALID, "near block %d: column is not a trial leaf", b);
             const int64_t nc = d.trial.value_ptr[col + 1] - d.trial.value_ptr[col];
-            if (d.near_offset[b] < 0 || d.near_offset[b] + nr * nc > d.near_len)
+            if (stored && (d.near_offset[b] < 0 || d.near_offset[b] + nr * nc > d.near_len))
                 return fail(H2B_ERR_INVALID, "near block %d exceeds the near array", b);
         }
     }
@@ -619,7 +669,7 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
             tr_off[b] = tr_len;
             tr_len += near_padded_ld(cplx, nc) * nr;
         }
-    c->near_entries = entries;
+    c->near_entries = d.near_kind == H2B_NEAR_STORED ? entries : 0;
     // groups over every output leaf, so that leaves without near blocks still get y = beta * y
     auto groups = [&](const h2b_side_desc &s, const std::vector<int> &key, std::vector<int> &leaf,
                       std::vector<int> &ptr, std::vector<int> &blk) {
@@ -639,6 +689,31 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
     int64_t *d_src_off;
     CUDA_TRY(c->upload(&d_row, blk_row.data(), blk_row.size()));
     CUDA_TRY(c->upload(&d_col, blk_col.data(), blk_col.size()));
+
+    if (d.near_kind != H2B_NEAR_STORED) {
+        // matrix-free: the block structure in both orientations, the points, no block data
+        DNear &dn = c->dnear;
+        dn.kind = d.near_kind;
+        dn.wavenumber = d.near_wavenumber;
+        double *pts;
+        CUDA_TRY(c->upload(&pts, d.test_points, (size_t)3 * std::max(d.test.ndofs, 1)));
+        dn.test_pts = pts;
+        CUDA_TRY(c->upload(&pts, d.trial_points, (size_t)3 * std::max(d.trial.ndofs, 1)));
+        dn.trial_pts = pts;
+        for (int side = 0; side < 2; ++side) {
+            std::vector<int> leaf, ptr, blk;
+            groups(side == 0 ? d.test : d.trial, side == 0 ? blk_row : blk_col, leaf, ptr, blk);
+            NearOp &op = side == 0 ? dn.fwd : dn.tr;
+            CUDA_TRY(c->upload(&p, leaf.data(), leaf.size())); op.grp_leaf = p;
+            CUDA_TRY(c->upload(&p, ptr.data(), ptr.size())); op.grp_ptr = p;
+            CUDA_TRY(c->upload(&p, blk.data(), blk.size())); op.grp_blk = p;
+            op.blk_in = side == 0 ? d_col : d_row;
+            op.ngroups = (int)leaf.size();
+        }
+        dn.symmetric = false;
+        CUDA_TRY(cudaDeviceSynchronize());
+        return H2B_OK;
+    }
     CUDA_TRY(c->upload(&d_src_off, src_off.data(), src_off.size()));
 
     // source blocks on the device (the caller's device buffer, or a temporary upload)
@@ -801,10 +876,16 @@ h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
             if (n0 == 0) continue;
             const int h0 = M.half_spectrum ? n0 / 2 + 1 : n0;
             const double *K = d.coupling + d.coupling_offset[k];
+            // a permuted coupling (PermutedTranslation) is expanded here: t[e] = canonical[perm[e]];
+            // the per-translation spectra are small next to the moments they multiply
+            const int32_t *pm = (d.coupling_rowperm && d.coupling_rowperm[k] >= 0)
+                                    ? d.coupling_perm + d.coupling_rowperm[k] : nullptr;
             for (int r = 0; r < n1 * n2; ++r)
                 for (int k1 = 0; k1 < h0; ++k1) {
-                    packed.push_back(K[2 * (k1 + (int64_t)n0 * r)]);
-                    packed.push_back(K[2 * (k1 + (int64_t)n0 * r) + 1]);
+                    const int64_t e = k1 + (int64_t)n0 * r;
+                    const int64_t src = pm ? pm[e] : e;
+                    packed.push_back(K[2 * src]);
+                    packed.push_back(K[2 * src + 1]);
                 }
         }
         if (packed.empty()) packed.assign(2, 0.0);
@@ -820,20 +901,62 @@ h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
     int64_t *q;
     CUDA_TRY(c->upload(&q, off.data(), off.size()));
     M.cpl_off = q;
+    // permuted dense couplings (PermutedDenseTranslation): the canonical blocks stay shared; per
+    // coupling a set [rowperm | rowperm^-1 | colperm | colperm^-1] (n each) that the I2O kernel
+    // reads through (identity where a permutation is absent)
+    std::vector<int64_t> perm_set;
+    if (!toep && d.coupling_rowperm && d.coupling_kind == H2B_COUPLING_DENSE) {
+        std::vector<int> sets;
+        std::map<std::tuple<int64_t, int64_t, int64_t>, int64_t> made;
+        perm_set.assign(std::max<int64_t>(d.ncouplings, 1), -1);
+        std::vector<int64_t> nk(std::max<int64_t>(d.ncouplings, 1), -1);  // square: n x n
+        for (const h2b_side_desc *sd : {&d.test, &d.trial})
+            for (int n = 0; n < sd->nnodes; ++n)
+                for (int p = sd->i2o_ptr[n]; p < sd->i2o_ptr[n + 1]; ++p)
+                    nk[sd->i2o_coupling[p]] = ncoef_host(*sd, sd->level[n]);
+        for (int64_t k = 0; k < d.ncouplings; ++k) {
+            const int64_t ro = d.coupling_rowperm[k], co = d.coupling_colperm[k], n = nk[k];
+            if ((ro < 0 && co < 0) || n < 0) continue;
+            auto it = made.find({ro, co, n});
+            if (it != made.end()) {
+                perm_set[k] = it->second;
+                continue;
+            }
+            const int64_t base = (int64_t)sets.size();
+            sets.resize(base + 4 * n);
+            for (int w = 0; w < 2; ++w) {
+                const int64_t o = w == 0 ? ro : co;
+                int *fw = sets.data() + base + 2 * w * n, *iv = fw + n;
+                for (int64_t i = 0; i < n; ++i) fw[i] = o >= 0 ? d.coupling_perm[o + i] : (int)i;
+                for (int64_t i = 0; i < n; ++i) iv[fw[i]] = (int)i;
+            }
+            made[{ro, co, n}] = base;
+            perm_set[k] = base;
+        }
+        if (sets.empty()) sets.assign(1, 0);
+        int *pq;
+        CUDA_TRY(c->upload(&pq, sets.data(), sets.size()));
+        M.perm = pq;
+    }
     // per-pair operand offsets for the I2O kernel (both sides; sources live on the other side)
     for (int side = 0; side < 2; ++side) {
         const h2b_side_desc &sd = side == 0 ? d.test : d.trial;
         SideHost &h = side == 0 ? c->test : c->trial;
         const SideHost &o = side == 0 ? c->trial : c->test;
         const int np = sd.i2o_ptr[sd.nnodes];
-        std::vector<int64_t> psrc(std::max(np, 1)), pcpl(std::max(np, 1));
+        std::vector<int64_t> psrc(std::max(np, 1)), pcpl(std::max(np, 1)), pperm(std::max(np, 1), -1);
         for (int p = 0; p < np; ++p) {
             const int src = sd.i2o_src[p];
             psrc[p] = toep ? o.spec_off_host[src] : o.mom_off_host[src];
             pcpl[p] = off[sd.i2o_coupling[p]];
+            if (!perm_set.empty()) pperm[p] = perm_set[sd.i2o_coupling[p]];
         }
         CUDA_TRY(c->upload(&q, psrc.data(), psrc.size())); h.d.pair_src = q;
         CUDA_TRY(c->upload(&q, pcpl.data(), pcpl.size())); h.d.pair_cpl = q;
+        if (!perm_set.empty()) {
+            CUDA_TRY(c->upload(&q, pperm.data(), pperm.size()));
+            h.d.pair_perm = q;
+        }
         if (toep) {
             st = build_sibling_groups(c, sd, h, o.spec_off_host, off);
             if (st) return st;

@@ -92,6 +92,7 @@ struct DSide {
     const int64_t *i2o_cpl;   // coupling index of each pair
     const int64_t *pair_src;  // per pair: the source's moment / spectrum offset per unit rhs
     const int64_t *pair_cpl;  // per pair: the coupling's element offset in the coupling array
+    const int64_t *pair_perm = nullptr;  // per pair: its permutation set in DMap::perm, -1 none
 };
 
 struct DMap {
@@ -101,6 +102,8 @@ struct DMap {
     int cube_ts;             // > 0: every level's padded Toeplitz arrays are cube_ts^3 (3-D cubes)
     const int64_t *cpl_off;  // [ncouplings] offsets in elements of T (dense/diag) or spectrum (Toeplitz)
     const void *cpl;
+    // permuted dense couplings: sets [rowperm | rowperm^-1 | colperm | colperm^-1], n entries each
+    const int *perm = nullptr;
 };
 
 // One oriented near operator: for every output leaf (group), the dense blocks that write its rows.
@@ -119,6 +122,11 @@ struct DNear {
     NearOp fwd;              // N: rows on the test side, columns on the trial side
     NearOp tr;               // N^T (unused when symmetric)
     bool symmetric = false;  // N^T == N: transposed products run on `fwd`
+    // matrix-free near field (kind != H2B_NEAR_STORED): entries from the points, no block data
+    int kind = 0;
+    double wavenumber = 0.0;
+    const double *test_pts = nullptr;   // [test ndofs * 3]
+    const double *trial_pts = nullptr;  // [trial ndofs * 3]
 };
 
 // Sibling groups for the Toeplitz I2O (i2o_sibling_kernel): the receiving children of one parent.

@@ -462,6 +462,123 @@ __global__ void __launch_bounds__(256) toeplitz_out_kernel(DMap m, DSide s, cons
     }
 }
 
+// Pruned transforms of real maps with 4-point cube moments (padded 7^3, half spectra 4 x 7 x 7):
+// the zero padding and the Hermitian half are never computed. In: the moment (4^3 reals) is
+// transformed along axis 0 into the 4 stored frequencies only (4^3 outputs), then along axis 1
+// (4 x 7 x 4) and axis 2 (4 x 7 x 7), each output a 4-term sum over the non-zero inputs; 1,488
+// complex multiply-adds against 7,203 for the three full line passes. Out: the inverse pass runs
+// axis 2 then axis 1 into the 4^3 corner only, and axis 0 rebuilds the real corner values from the
+// stored half, x[i] = Re Q[0] + 2 Re sum_{k=1..3} Q[k] w^{ki} (Q is Hermitian along axis 0 once
+// axes 1 and 2 are back in space). FP64 arithmetic; one transform per 64 threads.
+// ---------------------------------------------------------------------------------------------
+constexpr int PR_T = 64;   // threads per transform
+constexpr int PR_G = 4;    // transforms per CTA
+
+__device__ __forceinline__ void pr_twiddles(cdouble *tw, bool inverse) {
+    if (threadIdx.x < 7) {
+        double sv, cv;
+        sincospi(2.0 * threadIdx.x / 7.0, &sv, &cv);
+        tw[threadIdx.x] = {cv, inverse ? sv : -sv};
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(PR_T * PR_G)
+toeplitz_in_cube4_real_kernel(DSide s, const int *__restrict__ nodes, int ntrans, bool inverse, int nq,
+                              int nrhs, const T *__restrict__ am,
+                              typename ScalarTraits<T>::Complex *__restrict__ as) {
+    using S = typename ScalarTraits<T>::Complex;
+    __shared__ cdouble tw[7];
+    __shared__ double mom[PR_G][64];
+    __shared__ cdouble A[PR_G][64];   // [k1 < 4][i2 < 4][i3 < 4]
+    __shared__ cdouble B[PR_G][112];  // [k1 < 4][k2 < 7][i3 < 4]
+    const int grp = threadIdx.x / PR_T, tl = threadIdx.x % PR_T;
+    const int t = blockIdx.x * PR_G + grp;
+    const bool busy = t < ntrans;
+    const int node = busy ? nodes[t / nq] : nodes[0];
+    const int q = busy ? t % nq : 0;
+    pr_twiddles(tw, inverse);
+    if (busy) mom[grp][tl] = (double)am[s.mom_off[node] * nrhs + (int64_t)q * 64 + tl];
+    __syncthreads();
+    {  // axis 0: real inputs i1 < 4, stored frequencies k1 < 4
+        const int k1 = tl & 3, r = tl >> 2;
+        cdouble a = {0.0, 0.0};
+#pragma unroll
+        for (int i1 = 0; i1 < 4; ++i1) a = a + mom[grp][i1 + 4 * r] * tw[(k1 * i1) % 7];
+        A[grp][tl] = a;
+    }
+    __syncthreads();
+    for (int o = tl; o < 112; o += PR_T) {  // axis 1: inputs i2 < 4, all k2 < 7
+        const int k1 = o & 3, k2 = (o >> 2) % 7, i3 = o / 28;
+        cdouble b = {0.0, 0.0};
+#pragma unroll
+        for (int i2 = 0; i2 < 4; ++i2) b = b + A[grp][k1 + 4 * (i2 + 4 * i3)] * tw[(k2 * i2) % 7];
+        B[grp][o] = b;
+    }
+    __syncthreads();
+    if (busy) {  // axis 2: inputs i3 < 4, all k3 < 7; stored as [k1][k2][k3]
+        S *spec = as + s.spec_off[node] * nrhs + (int64_t)q * 196;
+        const double sc = inverse ? 1.0 / 343.0 : 1.0;
+        for (int o = tl; o < 196; o += PR_T) {
+            const int k12 = o % 28, k3 = o / 28;
+            cdouble c = {0.0, 0.0};
+#pragma unroll
+            for (int i3 = 0; i3 < 4; ++i3) c = c + B[grp][k12 + 28 * i3] * tw[(k3 * i3) % 7];
+            narrow(sc * c, spec[o]);
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(PR_T * PR_G)
+toeplitz_out_cube4_real_kernel(DSide s, const int *__restrict__ nodes, int ntrans, bool inverse, int nq,
+                               int nrhs, const typename ScalarTraits<T>::Complex *__restrict__ ds,
+                               T *__restrict__ dm) {
+    __shared__ cdouble tw[7];
+    __shared__ cdouble X[PR_G][196];  // stored half spectrum [k1 < 4][k2 < 7][k3 < 7]
+    __shared__ cdouble P[PR_G][112];  // [k1 < 4][k2 < 7][i3 < 4]
+    __shared__ cdouble Q[PR_G][64];   // [k1 < 4][i2 < 4][i3 < 4]
+    const int grp = threadIdx.x / PR_T, tl = threadIdx.x % PR_T;
+    const int t = blockIdx.x * PR_G + grp;
+    const bool busy = t < ntrans;
+    const int node = busy ? nodes[t / nq] : nodes[0];
+    const int q = busy ? t % nq : 0;
+    pr_twiddles(tw, inverse);
+    if (busy) {
+        const auto *spec = ds + s.spec_off[node] * nrhs + (int64_t)q * 196;
+        for (int o = tl; o < 196; o += PR_T) X[grp][o] = wide(spec[o]);
+    }
+    __syncthreads();
+    for (int o = tl; o < 112; o += PR_T) {  // axis 2 back to i3 < 4
+        const int k12 = o % 28, i3 = o / 28;
+        cdouble p = {0.0, 0.0};
+#pragma unroll
+        for (int k3 = 0; k3 < 7; ++k3) p = p + X[grp][k12 + 28 * k3] * tw[(k3 * i3) % 7];
+        P[grp][o] = p;
+    }
+    __syncthreads();
+    {  // axis 1 back to i2 < 4
+        const int k1 = tl & 3, i2 = (tl >> 2) & 3, i3 = tl >> 4;
+        cdouble v = {0.0, 0.0};
+#pragma unroll
+        for (int k2 = 0; k2 < 7; ++k2) v = v + P[grp][k1 + 4 * (k2 + 7 * i3)] * tw[(k2 * i2) % 7];
+        Q[grp][tl] = v;
+    }
+    __syncthreads();
+    if (busy) {  // axis 0 from the Hermitian half, real corner i1 < 4
+        const int i1 = tl & 3, r = tl >> 2;
+        const cdouble *qv = &Q[grp][4 * r];
+        double x = qv[0].x;
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1) {
+            const cdouble w = tw[(k1 * i1) % 7];
+            x += 2.0 * (qv[k1].x * w.x - qv[k1].y * w.y);
+        }
+        const double sc = inverse ? 1.0 / 343.0 : 1.0;
+        narrow(sc * x, dm[s.mom_off[node] * nrhs + (int64_t)q * 64 + tl]);
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // B1/B2: l_r = sum over pairs of op(B_key) m_t (dense), d .* m_t (diagonal), or, for Toeplitz,
 // S_r = sum K_key .* S_t on the spectra. op: identity / transpose / adjoint by map orientation
@@ -555,9 +672,28 @@ __global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, cons
                 const int snc = ncoef_of(t, t.level[r.i2o_src[p]]);
                 const T *B = B0 + r.pair_cpl[p];
                 const T *X = am + r.pair_src[p] * nrhs;
-                // forward: block (r, t) is nc x snc; transposed: block (t, r) is snc x nc
-                tile_gemm(B, mode == H2B_FORWARD ? nc : snc, mode != H2B_FORWARD, adj, m0, mt, snc, nqc,
-                          [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + k]); }, Ms, Xs, acc);
+                const int64_t ps = r.pair_perm ? r.pair_perm[p] : -1;
+                if (ps < 0) {
+                    // forward: block (r, t) is nc x snc; transposed: block (t, r) is snc x nc
+                    tile_gemm(B, mode == H2B_FORWARD ? nc : snc, mode != H2B_FORWARD, adj, m0, mt, snc, nqc,
+                              [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + k]); }, Ms, Xs, acc);
+                } else if (mode == H2B_FORWARD) {
+                    // t[rp[i], cp[j]] = M[i, j]: out[i] += sum_j M[rp^-1[i], j] x[cp[j]]
+                    // (gather / canonical product / scatter of symmetryreduceddense.jl:84-95,
+                    // with the scatter folded into the row index)
+                    const int *ri = m.perm + ps + nc, *cp = m.perm + ps + 2 * nc;
+                    tile_gemm_l(false, m0, mt, snc, nqc,
+                                [&](int i, int k) -> A { return wide(cj(B[ri[i] + (int64_t)k * nc], adj)); },
+                                [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + cp[k]]); },
+                                Ms, Xs, acc);
+                } else {
+                    // transposed / adjoint: out[j] += sum_i op(M)[cp^-1[j], i] x[rp[i]]
+                    const int *rp = m.perm + ps, *ci = m.perm + ps + 3 * snc;
+                    tile_gemm_l(true, m0, mt, snc, nqc,
+                                [&](int i, int k) -> A { return wide(cj(B[k + (int64_t)ci[i] * snc], adj)); },
+                                [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + rp[k]]); },
+                                Ms, Xs, acc);
+                }
             }
 #pragma unroll
             for (int j = 0; j < TG_O; ++j) {
@@ -591,16 +727,19 @@ i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
     const bool adj = mode == H2B_ADJOINT;
     const S *K0 = static_cast<const S *>(m.cpl);
     const int k0 = g.ptr[gi], k1 = g.ptr[gi + 1];
-    cdouble acc[8][QB];
+    // accumulated in the storage type: FP64 in the FP64 form; FP32 in the FP32 form, whose sums of
+    // at most one interaction list (189 pairs in a uniform tree) per frequency keep the product
+    // within 3.2e-7 of the FP64 one on the benchmark map (2.2e-7 with FP64 sums)
+    S acc[8][QB];
 #pragma unroll
     for (int sl = 0; sl < 8; ++sl)
 #pragma unroll
-        for (int q = 0; q < QB; ++q) acc[sl][q] = cdouble{0.0, 0.0};
+        for (int q = 0; q < QB; ++q) acc[sl][q] = S{};
     // U source entries per step (two for one right-hand side, where registers allow), every load
     // issued before the arithmetic that uses it
     constexpr int U = QB == 1 ? 2 : 1;
     for (int k = k0; k < k1; k += U) {
-        cdouble sv[U][QB];
+        S sv[U][QB];
         int ko[U][8];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -610,7 +749,7 @@ i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
             for (int sl = 0; sl < 8; ++sl) ko[u][sl] = ok ? kof[sl] : -1;
             const S *sp = as + g.src_off[ok ? k + u : k] * nrhs + (int64_t)q0 * slen + e;
 #pragma unroll
-            for (int q = 0; q < QB; ++q) sv[u][q] = q0 + q < nq ? wide(sp[(int64_t)q * slen]) : cdouble{0.0, 0.0};
+            for (int q = 0; q < QB; ++q) sv[u][q] = q0 + q < nq ? sp[(int64_t)q * slen] : S{};
         }
         S kvs[U][8];
 #pragma unroll
@@ -622,7 +761,7 @@ i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
 #pragma unroll
             for (int sl = 0; sl < 8; ++sl) {
                 if (ko[u][sl] >= 0) {
-                    const cdouble kv = wide(cj(kvs[u][sl], adj));
+                    const S kv = cj(kvs[u][sl], adj);
 #pragma unroll
                     for (int q = 0; q < QB; ++q) acc[sl][q] = acc[sl][q] + kv * sv[u][q];
                 }
@@ -635,7 +774,7 @@ i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
         S *out = ds + r.spec_off[rv] * nrhs + (int64_t)q0 * slen + e;
 #pragma unroll
         for (int q = 0; q < QB; ++q)
-            if (q0 + q < nq) narrow(acc[sl][q], out[(int64_t)q * slen]);
+            if (q0 + q < nq) out[(int64_t)q * slen] = acc[sl][q];
     }
 }
 
@@ -815,6 +954,33 @@ int fft_groups(int maxt, size_t scalar) {
 }
 }  // namespace
 
+// the pruned real-map transforms (complex maps keep the general ones)
+template <class T>
+cudaError_t launch_pruned_in(const DSide &s, const int *nodes, int ntrans, bool inverse, int nq,
+                             const FarArgs &fa, cudaStream_t st) {
+    if constexpr (ScalarTraits<T>::is_complex) {
+        return cudaErrorInvalidValue;
+    } else {
+        using S = typename ScalarTraits<T>::Complex;
+        toeplitz_in_cube4_real_kernel<T><<<(ntrans + PR_G - 1) / PR_G, PR_T * PR_G, 0, st>>>(
+            s, nodes, ntrans, inverse, nq, fa.nrhs, static_cast<const T *>(fa.am), static_cast<S *>(fa.as));
+        return cudaGetLastError();
+    }
+}
+
+template <class T>
+cudaError_t launch_pruned_out(const DSide &s, const int *nodes, int ntrans, bool inverse, int nq,
+                              const FarArgs &fa, cudaStream_t st) {
+    if constexpr (ScalarTraits<T>::is_complex) {
+        return cudaErrorInvalidValue;
+    } else {
+        using S = typename ScalarTraits<T>::Complex;
+        toeplitz_out_cube4_real_kernel<T><<<(ntrans + PR_G - 1) / PR_G, PR_T * PR_G, 0, st>>>(
+            s, nodes, ntrans, inverse, nq, fa.nrhs, static_cast<const S *>(fa.ds), static_cast<T *>(fa.dm));
+        return cudaGetLastError();
+    }
+}
+
 cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DSide &s,
                                const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
                                int maxtsize, int maxaxis, cudaStream_t st) {
@@ -836,6 +1002,10 @@ cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DS
                     m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const T *>(fa.am), static_cast<S *>(fa.as));
             return e2;
         };
+        if (!cplx && cube7 && m.half_spectrum) {
+            err = launch_pruned_in<T>(s, nodes, ntrans, inverse, m.ncomp * fa.nrhs, fa, st);
+            break;
+        }
         err = cube7 ? launch(toeplitz_in_kernel<T, 7, 7>)
                     : (maxaxis <= 7 ? launch(toeplitz_in_kernel<T, 7, 0>) : launch(toeplitz_in_kernel<T, 15, 0>));
     });
@@ -863,6 +1033,10 @@ cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const D
                     m, s, nodes, ntrans, inverse, fa.nrhs, maxtsize, static_cast<const S *>(fa.ds), static_cast<T *>(fa.dm));
             return e2;
         };
+        if (!cplx && cube7 && m.half_spectrum) {
+            err = launch_pruned_out<T>(s, nodes, ntrans, inverse, m.ncomp * fa.nrhs, fa, st);
+            break;
+        }
         err = cube7 ? launch(toeplitz_out_kernel<T, 7, 7>)
                     : (maxaxis <= 7 ? launch(toeplitz_out_kernel<T, 7, 0>) : launch(toeplitz_out_kernel<T, 15, 0>));
     });
@@ -896,13 +1070,15 @@ cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const D
     const int bs = block_for(maxslen, 32, 512);
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
-        // two right-hand sides per CTA share each kernel value load (one-wide blocks reload them
-        // per right-hand side, which costs more than the lower occupancy of the wider block)
+        // several right-hand sides per CTA share each kernel value load (one-wide blocks reload
+        // them per right-hand side, which costs more than the lower occupancy of the wider block):
+        // four with FP32 accumulators, two with FP64 ones (four would spill)
+        constexpr int QB = sizeof(typename ScalarTraits<T>::Real) == 4 ? 4 : 2;
         if (nq == 1)
             i2o_sibling_kernel<T, 1><<<dim3(g.ngroups, 1), bs, 0, st>>>(
                 m, recv, g, fa.mode, fa.nrhs, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
         else
-            i2o_sibling_kernel<T, 2><<<dim3(g.ngroups, (nq + 1) / 2), bs, 0, st>>>(
+            i2o_sibling_kernel<T, QB><<<dim3(g.ngroups, (nq + QB - 1) / QB), bs, 0, st>>>(
                 m, recv, g, fa.mode, fa.nrhs, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
     });
     return cudaGetLastError();

@@ -65,14 +65,18 @@ __device__ __forceinline__ int near_ld(int nr, double *) { return nr + (nr & 1);
 __device__ __forceinline__ int near_ld(int nr, cdouble *) { return nr; }
 
 // y[rows(g)] = alpha * op(N_g) x + beta * y[rows(g)] for right-hand sides [r0, r0 + R).
+// A pass covers MP chunks of 32 * RPL rows, so a leaf of up to 32 * RPL * MP rows takes a single
+// sweep over its blocks (one x gather per column chunk, no column split between passes). UB
+// columns are loaded before any is used.
 // Shared memory: per warp, the x values of its current 32-column chunk ([32][R]), read back as
 // broadcasts; then the warps' partial rows ([NEAR_WARPS][RPP][R]) for the final reduction.
-template <class V, int R>
-__global__ void __launch_bounds__(NEAR_WARPS * 32, 2)
+template <class V, int R, int MP, int UB, int MINB>
+__global__ void __launch_bounds__(NEAR_WARPS * 32, MINB)
 near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, const V *__restrict__ x,
                  int64_t ldx, V *__restrict__ y, int64_t ldy, V alpha, V beta, bool beta_zero) {
     constexpr int RPL = NearVec<V>::RPL;
-    constexpr int RPP = 32 * RPL;  // rows per pass
+    constexpr int RPC = 32 * RPL;  // rows per chunk
+    constexpr int RPP = RPC * MP;  // rows per pass
     extern __shared__ unsigned char smem_raw[];
     const int g = blockIdx.x;
     const int leaf = op.grp_leaf[g];
@@ -84,13 +88,21 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
     const V *D = static_cast<const V *>(op.data);
     const int ld = near_ld(nr, (V *)nullptr);
     for (int p0 = 0; p0 < nr; p0 += RPP) {
-        const int i0 = p0 + RPL * lane;  // first row of this lane
-        const bool live = i0 < nr;       // lanes past the last row load nothing
-        V acc[RPL][R];
+        const int i0 = p0 + RPL * lane;  // first row of this lane in chunk 0
+        bool live[MP];                   // lanes past the last row load nothing
+        bool any[MP];                    // warp-uniform: the chunk has rows at all
 #pragma unroll
-        for (int k = 0; k < RPL; ++k)
+        for (int c = 0; c < MP; ++c) {
+            live[c] = i0 + c * RPC < nr;
+            any[c] = p0 + c * RPC < nr;
+        }
+        V acc[MP][RPL][R];
 #pragma unroll
-            for (int q = 0; q < R; ++q) acc[k][q] = V{};
+        for (int c = 0; c < MP; ++c)
+#pragma unroll
+            for (int k = 0; k < RPL; ++k)
+#pragma unroll
+                for (int q = 0; q < R; ++q) acc[c][k][q] = V{};
         // work units are (block, 32-column chunk) pairs, dealt round-robin to the warps
         int unit = 0;
         for (int bb = b0; bb < b1; ++bb) {
@@ -112,48 +124,61 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
                 const int jn = min(32, nc - j0);
                 const V *Bj = B + (int64_t)j0 * ld;
                 int jj = 0;
-                for (; jj + 8 <= jn; jj += 8) {
-                    V bv[8][RPL];  // eight columns in flight before any use
+                for (; jj + UB <= jn; jj += UB) {
+                    V bv[UB][MP][RPL];  // UB columns in flight before any use
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        if (live) {
-                            load_rows(Bj + (int64_t)(jj + u) * ld, bv[u]);
-                        } else {
+                    for (int u = 0; u < UB; ++u)
 #pragma unroll
-                            for (int k = 0; k < RPL; ++k) bv[u][k] = V{};
+                        for (int c = 0; c < MP; ++c) {
+                            if (live[c]) {
+                                load_rows(Bj + (int64_t)(jj + u) * ld + c * RPC, bv[u][c]);
+                            } else {
+#pragma unroll
+                                for (int k = 0; k < RPL; ++k) bv[u][c][k] = V{};
+                            }
                         }
-                    }
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
+                    for (int u = 0; u < UB; ++u) {
                         V xv[R];
                         load_x<V, R>(xs + (jj + u) * R, xv);
 #pragma unroll
-                        for (int q = 0; q < R; ++q)
+                        for (int c = 0; c < MP; ++c) {
+                            if (!any[c]) continue;
 #pragma unroll
-                            for (int k = 0; k < RPL; ++k) acc[k][q] = fma_c(bv[u][k], xv[q], acc[k][q], cjg);
+                            for (int q = 0; q < R; ++q)
+#pragma unroll
+                                for (int k = 0; k < RPL; ++k)
+                                    acc[c][k][q] = fma_c(bv[u][c][k], xv[q], acc[c][k][q], cjg);
+                        }
                     }
                 }
                 for (; jj < jn; ++jj) {
-                    V bv[RPL];
-                    if (live) {
-                        load_rows(Bj + (int64_t)jj * ld, bv);
-                    } else {
 #pragma unroll
-                        for (int k = 0; k < RPL; ++k) bv[k] = V{};
-                    }
+                    for (int c = 0; c < MP; ++c) {
+                        if (!any[c]) continue;
+                        V bv[RPL];
+                        if (live[c]) {
+                            load_rows(Bj + (int64_t)jj * ld + c * RPC, bv);
+                        } else {
 #pragma unroll
-                    for (int q = 0; q < R; ++q) {
-                        const V xv = xs[jj * R + q];
+                            for (int k = 0; k < RPL; ++k) bv[k] = V{};
+                        }
 #pragma unroll
-                        for (int k = 0; k < RPL; ++k) acc[k][q] = fma_c(bv[k], xv, acc[k][q], cjg);
+                        for (int q = 0; q < R; ++q) {
+                            const V xv = xs[jj * R + q];
+#pragma unroll
+                            for (int k = 0; k < RPL; ++k) acc[c][k][q] = fma_c(bv[k], xv, acc[c][k][q], cjg);
+                        }
                     }
                 }
             }
         }
 #pragma unroll
-        for (int k = 0; k < RPL; ++k)
+        for (int c = 0; c < MP; ++c)
 #pragma unroll
-            for (int q = 0; q < R; ++q) part[(warp * RPP + RPL * lane + k) * R + q] = acc[k][q];
+            for (int k = 0; k < RPL; ++k)
+#pragma unroll
+                for (int q = 0; q < R; ++q) part[(warp * RPP + c * RPC + RPL * lane + k) * R + q] = acc[c][k][q];
         __syncthreads();
         const int rows = min(RPP, nr - p0);
         for (int e = threadIdx.x; e < rows * rc; e += blockDim.x) {
@@ -278,6 +303,163 @@ cudaError_t launch_rows_mma(const NearOp &op, const DSide &outs, const DSide &in
     return cudaGetLastError();
 }
 
+// Matrix-free near field ---------------------------------------------------------------------
+// The point kernels of H2B_NEAR_LAPLACE / H2B_NEAR_HELMHOLTZ: the entry of (output dof i, input
+// dof j) from their squared distance; 0 for coincident points (the self term).
+constexpr double kInv4Pi = 0.25 / 3.141592653589793;
+
+template <int KIND, class V> __device__ __forceinline__ V near_entry(double r2, double k);
+template <> __device__ __forceinline__ double near_entry<H2B_NEAR_LAPLACE, double>(double r2, double) {
+    return r2 > 0.0 ? kInv4Pi * rsqrt(r2) : 0.0;
+}
+template <> __device__ __forceinline__ cdouble near_entry<H2B_NEAR_LAPLACE, cdouble>(double r2, double) {
+    return {r2 > 0.0 ? kInv4Pi * rsqrt(r2) : 0.0, 0.0};
+}
+template <> __device__ __forceinline__ cdouble near_entry<H2B_NEAR_HELMHOLTZ, cdouble>(double r2, double k) {
+    if (!(r2 > 0.0)) return {0.0, 0.0};
+    const double r = sqrt(r2);
+    double sn, cs;
+    sincos(k * r, &sn, &cs);
+    const double w = kInv4Pi / r;
+    return {cs * w, sn * w};
+}
+
+// y[rows(g)] = alpha * op(N_g) x + beta * y[rows(g)] with N's entries computed from the points:
+// the block walk of near_rows_kernel (units = (block, 32-column chunk) dealt to the warps), but
+// each lane owns rows lane, lane + 32, ... (up to RM per pass, as many as the leaf needs) and
+// evaluates its entries column by column; the column's point and x values are broadcast from
+// shared memory. N^T has the same entries with the roles of the sides swapped (the kernels are
+// symmetric), conj(N^T) for adjoint maps.
+template <class V, int KIND, int R, int RM>
+__global__ void __launch_bounds__(NEAR_WARPS * 32, 2)
+near_free_kernel(NearOp op, DSide outs, DSide ins, const double *__restrict__ pout,
+                 const double *__restrict__ pin, double wavenumber, bool cjg, int r0, int rc,
+                 const V *__restrict__ x, int64_t ldx, V *__restrict__ y, int64_t ldy, V alpha, V beta,
+                 bool beta_zero) {
+    constexpr int RPP = 32 * RM;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int g = blockIdx.x;
+    const int leaf = op.grp_leaf[g];
+    const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
+    const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    V *xs = reinterpret_cast<V *>(smem_raw) + warp * 32 * R;             // this warp's x chunk
+    double *qs = reinterpret_cast<double *>(reinterpret_cast<V *>(smem_raw) + NEAR_WARPS * 32 * R) +
+                 warp * 32 * 3;                                             // its column points
+    V *part = reinterpret_cast<V *>(reinterpret_cast<double *>(reinterpret_cast<V *>(smem_raw) +
+                                                               NEAR_WARPS * 32 * R) + NEAR_WARPS * 32 * 3);
+    for (int p0 = 0; p0 < nr; p0 += RPP) {
+        const int km = min(RM, (nr - p0 + 31) / 32);  // warp-uniform: row slots in use
+        double px[RM], py[RM], pz[RM];
+        bool live[RM];
+        V acc[RM][R];
+#pragma unroll
+        for (int k = 0; k < RM; ++k) {
+            const int i = p0 + 32 * k + lane;
+            live[k] = i < nr;
+            const int64_t dof = live[k] ? outs.value[o0 + i] : outs.value[o0];
+            px[k] = pout[3 * dof];
+            py[k] = pout[3 * dof + 1];
+            pz[k] = pout[3 * dof + 2];
+#pragma unroll
+            for (int q = 0; q < R; ++q) acc[k][q] = V{};
+        }
+        int unit = 0;
+        for (int bb = b0; bb < b1; ++bb) {
+            const int blk = op.grp_blk[bb];
+            const int inl = op.blk_in[blk];
+            const int c0 = ins.value_ptr[inl], nc = ins.value_ptr[inl + 1] - c0;
+            for (int j0 = 0; j0 < nc; j0 += 32, ++unit) {
+                if (unit % NEAR_WARPS != warp) continue;
+                __syncwarp();
+                {
+                    const int jl = j0 + lane;
+                    const int64_t dof = jl < nc ? ins.value[c0 + jl] : 0;
+#pragma unroll
+                    for (int q = 0; q < R; ++q)
+                        xs[lane * R + q] = (jl < nc && q < rc) ? x[(int64_t)(r0 + q) * ldx + dof] : V{};
+                    qs[3 * lane] = pin[3 * dof];
+                    qs[3 * lane + 1] = pin[3 * dof + 1];
+                    qs[3 * lane + 2] = pin[3 * dof + 2];
+                }
+                __syncwarp();
+                const int jn = min(32, nc - j0);
+                for (int jj = 0; jj < jn; ++jj) {
+                    const double qx = qs[3 * jj], qy = qs[3 * jj + 1], qz = qs[3 * jj + 2];
+                    V xv[R];
+                    load_x<V, R>(xs + jj * R, xv);
+#pragma unroll
+                    for (int k = 0; k < RM; ++k) {
+                        if (k >= km) break;
+                        const double dx = px[k] - qx, dy = py[k] - qy, dz = pz[k] - qz;
+                        const V a = near_entry<KIND, V>(fma(dx, dx, fma(dy, dy, dz * dz)), wavenumber);
+#pragma unroll
+                        for (int q = 0; q < R; ++q) acc[k][q] = fma_c(a, xv[q], acc[k][q], cjg);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RM; ++k)
+#pragma unroll
+            for (int q = 0; q < R; ++q) part[(warp * RPP + 32 * k + lane) * R + q] = acc[k][q];
+        __syncthreads();
+        const int rows = min(RPP, nr - p0);
+        for (int e = threadIdx.x; e < rows * rc; e += blockDim.x) {
+            const int i = e / rc, q = e % rc;
+            V s = V{};
+#pragma unroll
+            for (int w = 0; w < NEAR_WARPS; ++w) s = s + part[(w * RPP + i) * R + q];
+            V *o = &y[(int64_t)(r0 + q) * ldy + outs.value[o0 + p0 + i]];
+            const V v = alpha * s;
+            *o = beta_zero ? v : v + beta * *o;
+        }
+        __syncthreads();
+    }
+}
+
+// rows per lane and pass: four (128 rows) for one or two right-hand sides, fewer where the
+// accumulators of more right-hand sides need the registers
+template <class V, int R> struct FreeShape {
+    static constexpr bool cplx = sizeof(V) == 16;
+    static constexpr int RM = R <= 2 ? 4 : (R <= 8 && !cplx ? 2 : (R <= 4 ? 2 : 1));
+};
+
+template <class V, int KIND, int R>
+cudaError_t launch_free_t(const NearOp &op, const DSide &outs, const DSide &ins, const double *pout,
+                          const double *pin, double k, bool cjg, int r0, int rc, const V *x, int64_t ldx,
+                          V *y, int64_t ldy, V alpha, V beta, bool bz, cudaStream_t st) {
+    constexpr int RM = FreeShape<V, R>::RM;
+    const size_t sm = (size_t)NEAR_WARPS * (32 * R * sizeof(V) + 32 * 3 * sizeof(double) +
+                                            (size_t)32 * RM * R * sizeof(V));
+    auto kern = near_free_kernel<V, KIND, R, RM>;
+    cudaError_t e = cudaSuccess;
+    if (sm > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    kern<<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, pout, pin, k, cjg, r0, rc, x, ldx, y, ldy,
+                                                   alpha, beta, bz);
+    return cudaGetLastError();
+}
+
+template <class V, int KIND>
+cudaError_t near_free_apply_t(const NearOp &op, const DSide &outs, const DSide &ins, const double *pout,
+                              const double *pin, double k, bool cjg, int nrhs, const V *x, int64_t ldx,
+                              V *y, int64_t ldy, V alpha, V beta, bool bz, cudaStream_t st) {
+    if (op.ngroups == 0) return cudaSuccess;
+    constexpr int RB = sizeof(V) == 16 ? 8 : 16;  // complex: 16 accumulators would spill
+    for (int r0 = 0; r0 < nrhs; r0 += RB) {
+        const int rc = std::min(RB, nrhs - r0);
+        cudaError_t e;
+        if (rc == 1) e = launch_free_t<V, KIND, 1>(op, outs, ins, pout, pin, k, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        else if (rc == 2) e = launch_free_t<V, KIND, 2>(op, outs, ins, pout, pin, k, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        else if (rc <= 4) e = launch_free_t<V, KIND, 4>(op, outs, ins, pout, pin, k, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        else if (rc <= 8) e = launch_free_t<V, KIND, 8>(op, outs, ins, pout, pin, k, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        else e = launch_free_t<V, KIND, RB>(op, outs, ins, pout, pin, k, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // Build-time helpers --------------------------------------------------------------------------
 // Copy block b (nr x nc, column-major, leading dimension nr) into the padded layout; with
 // `transpose`, write its transpose (nc x nr) instead.
@@ -330,18 +512,29 @@ __global__ void near_symcheck_kernel(const V *__restrict__ src, const int64_t *_
     if (!__syncthreads_and(ok) && threadIdx.x == 0) *flag = 0;
 }
 
+// Pass shape per (field, right-hand sides): MP chunks per pass, UB columns per load batch, MINB
+// CTAs per SM for the register budget. Two right-hand sides take two chunks per pass (128 real or
+// 64 complex rows); one real right-hand side keeps one chunk and three CTAs per SM (85 registers),
+// which streams faster on B200 than the two-chunk pass at two CTAs per SM.
+template <class V, int R> struct NearShape {
+    static constexpr bool cplx = sizeof(V) == 16;
+    static constexpr int MP = R <= 2 ? 2 - (!cplx && R == 1) : 1;
+    static constexpr int UB = cplx ? 4 : 8;
+    static constexpr int MINB = 2;
+};
+
 template <class V, int R>
 cudaError_t launch_rows_t(const NearOp &op, const DSide &outs, const DSide &ins, bool cjg, int r0,
                           int rc, const V *x, int64_t ldx, V *y, int64_t ldy, V alpha, V beta,
                           bool bz, cudaStream_t st) {
-    constexpr int RPP = 32 * NearVec<V>::RPL;
+    constexpr int MP = NearShape<V, R>::MP, UB = NearShape<V, R>::UB, MINB = NearShape<V, R>::MINB;
+    constexpr int RPP = 32 * NearVec<V>::RPL * MP;
     const size_t sm = (size_t)NEAR_WARPS * (32 + RPP) * R * sizeof(V);
+    auto kern = near_rows_kernel<V, R, MP, UB, MINB>;
     cudaError_t e = cudaSuccess;
-    if (sm > 48 * 1024)
-        e = cudaFuncSetAttribute(near_rows_kernel<V, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (sm > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    near_rows_kernel<V, R><<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, cjg, r0, rc, x, ldx, y,
-                                                                     ldy, alpha, beta, bz);
+    kern<<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, cjg, r0, rc, x, ldx, y, ldy, alpha, beta, bz);
     return cudaGetLastError();
 }
 
@@ -416,6 +609,23 @@ cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &test, 
     const DSide &outs = fwd_op ? test : trial;
     const DSide &ins = fwd_op ? trial : test;
     const bool cjg = mode == H2B_ADJOINT && cplx;
+    if (n.kind != H2B_NEAR_STORED) {
+        const double *pout = fwd_op ? n.test_pts : n.trial_pts;
+        const double *pin = fwd_op ? n.trial_pts : n.test_pts;
+        const bool bz = beta.x == 0.0 && beta.y == 0.0;
+        const cdouble *xc = static_cast<const cdouble *>(x);
+        cdouble *yc = static_cast<cdouble *>(y);
+        if (n.kind == H2B_NEAR_HELMHOLTZ)
+            return near_free_apply_t<cdouble, H2B_NEAR_HELMHOLTZ>(op, outs, ins, pout, pin, n.wavenumber, cjg,
+                                                                   nrhs, xc, ldx, yc, ldy, alpha, beta, bz, st);
+        if (cplx)
+            return near_free_apply_t<cdouble, H2B_NEAR_LAPLACE>(op, outs, ins, pout, pin, 0.0, cjg, nrhs, xc,
+                                                                 ldx, yc, ldy, alpha, beta, bz, st);
+        return near_free_apply_t<double, H2B_NEAR_LAPLACE>(op, outs, ins, pout, pin, 0.0, false, nrhs,
+                                                            static_cast<const double *>(x), ldx,
+                                                            static_cast<double *>(y), ldy, alpha.x, beta.x,
+                                                            beta.x == 0.0, st);
+    }
     if (cplx)
         return near_apply_t<cdouble>(op, outs, ins, cjg, nrhs, static_cast<const cdouble *>(x), ldx,
                                      static_cast<cdouble *>(y), ldy, alpha, beta,

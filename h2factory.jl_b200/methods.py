@@ -102,6 +102,13 @@ def _axis_factors(nodes: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     return lo, hi
 
 
+def _grid_at(center, h, nodes, dim) -> np.ndarray:
+    """Interpolation points of a box (centre, half size), ordered like the moment coefficients."""
+    axes = [center[d] + h * nodes for d in range(dim)]
+    grids = np.meshgrid(*axes, indexing="ij")
+    return np.stack([g.ravel(order="F") for g in grids], axis=1).reshape(nodes.size ** dim, dim)
+
+
 def _node_grid(tree: Tree, n: int, nodes: np.ndarray) -> np.ndarray:
     """Interpolation points of box n, ordered like the moment coefficients."""
     p = nodes.size
@@ -112,10 +119,64 @@ def _node_grid(tree: Tree, n: int, nodes: np.ndarray) -> np.ndarray:
     return np.stack([g.ravel(order="F") for g in grids], axis=1).reshape(p ** tree.dim, tree.dim)
 
 
+def cube_symmetry(offs) -> tuple:
+    """Canonical representative of an integer offset under the signed axis permutations, and
+    the element (perm, signs) with offs = S c, (S v)_a = signs[a] * v[perm[a]].
+
+    The canonical offset sorts the absolute components in descending order, so the up to 48
+    offsets of one orbit (H2Trees' LatticeSymmetry group of the cube) share it.
+    """
+    offs = np.asarray(offs, np.int64)
+    a = np.abs(offs)
+    order = np.argsort(-a, kind="stable")
+    canon = a[order]
+    perm = np.empty_like(order)
+    perm[order] = np.arange(order.size)      # canon[perm[a]] == |offs[a]|
+    signs = np.where(offs < 0, -1, 1)
+    return canon, perm, signs
+
+
+def grid_permutation(p: int, dim: int, perm, signs) -> np.ndarray:
+    """Node permutation of a p^dim interpolation grid under S: index of S xi_i for each i.
+
+    Nodes symmetric about the box centre (xi_{p-1-k} = -xi_k, Chebyshev and equispaced) make
+    a sign flip the index reversal k -> p - 1 - k (symmetryreducedcollection.jl:197-230).
+    Coefficient order: axis 0 fastest.
+    """
+    idx = np.indices((p,) * dim).reshape(dim, -1)   # idx[a, lin] with axis 0 fastest below
+    lin = np.ravel_multi_index(idx[::-1], (p,) * dim)  # C order over reversed axes = axis 0 fastest
+    out = np.empty(p ** dim, np.int32)
+    img = np.empty_like(idx)
+    for a in range(dim):
+        comp = idx[perm[a]]
+        img[a] = comp if signs[a] > 0 else p - 1 - comp
+    out[lin] = np.ravel_multi_index(img[::-1], (p,) * dim)
+    return out
+
+
+def toeplitz_permutation(ts: int, dim: int, perm, signs) -> np.ndarray:
+    """Sample permutation of a padded (2p-1)^dim wrap-around tensor under S:
+    t_{S d}[j] = t_d[perm[j]], the wrap position of S^-1 m_j (symmetryreducedcollection.jl:150-195).
+    Valid for the FFT'd tensor too (S is orthogonal)."""
+    idx = np.indices((ts,) * dim).reshape(dim, -1)
+    signed = np.where(idx > ts // 2, idx - ts, idx)
+    inv = np.empty(dim, np.int64)
+    inv[np.asarray(perm)] = np.arange(dim)
+    src = np.empty_like(signed)
+    for b in range(dim):  # (S^-1 u)_b = signs[inv[b]] * u[inv[b]]
+        src[b] = signs[inv[b]] * signed[inv[b]]
+    src = np.mod(src, ts)
+    lin = np.ravel_multi_index(idx[::-1], (ts,) * dim)
+    out = np.empty(ts ** dim, np.int32)
+    out[lin] = np.ravel_multi_index(src[::-1], (ts,) * dim)
+    return out
+
+
 def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
                        transfers: str = "dense", couplings: str = "dense",
                        field: str | None = None, precision: str = "fp64",
-                       near: str = "host", alpha=1.0, trial: Tree | None = None) -> H2Core:
+                       near: str = "host", alpha=1.0, trial: Tree | None = None,
+                       symmetry: bool = False) -> H2Core:
     """H2 core of an interpolation FMM of order `p` for `kernel`.
 
     `tree` holds the test (row) points; `trial` the trial (column) points of a Petrov map
@@ -124,7 +185,11 @@ def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
     couplings = "dense" stores one M2L block per unique translation; "toeplitz" stores the
     FFT'd wrap-around kernel per unique translation (equispaced nodes, same-size boxes only).
     near = "host" assembles near blocks on the host; "none" leaves them to the caller
-    (e.g. assembled on the device, see h2factory_b200.assembly).
+    (e.g. assembled on the device, see h2factory_b200.assembly); "free" computes the near entries
+    on the device from the points (matrix-free; `laplace` and `helmholtz` kernels only).
+    symmetry = True stores one coupling per orbit of the cube's signed axis permutations and
+    reads the others through permutations (symmetry-reduced M2L, symmetryreduceddense.jl and
+    symmetryreducedcollection.jl); it needs a radial kernel and cube moments.
     """
     xi = chebyshev_nodes(p) if nodes == "chebyshev" else equispaced_nodes(p)
     if couplings == "toeplitz" and nodes != "equispaced":
@@ -173,7 +238,41 @@ def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
                            trial.level[far[:, 1]][:, None].astype(np.int64), offs], axis=1)
     ukeys, first, inv = np.unique(keys, axis=0, return_index=True, return_inverse=True)
     blocks = []
-    for u in range(ukeys.shape[0]):
+    canon_of = rowperms = colperms = None
+    if symmetry:
+        canon_of, rowperms, colperms, cache = [], [], [], {}
+        for u in range(ukeys.shape[0]):
+            lr, lt = int(ukeys[u, 0]), int(ukeys[u, 1])
+            c, prm, sg = cube_symmetry(ukeys[u, 2:])
+            ck = (lr, lt, *c.tolist())
+            if ck not in cache:
+                cache[ck] = len(blocks)
+                r, t = int(far[first[u], 0]), int(far[first[u], 1])
+                hr, ht = test.halfsize[r], trial.halfsize[t]
+                hmn = min(hr, ht)
+                # canonical geometry: receiver at the origin, source at offset c (units hmin / 2)
+                dc = -(hmn / 2.0) * c.astype(np.float64)
+                if couplings == "toeplitz":
+                    ts = 2 * p - 1
+                    m = np.arange(ts)
+                    m = np.where(m < p, m, m - ts)
+                    grids = np.meshgrid(*([m] * dim), indexing="ij")
+                    z = np.stack([dc[d] + (2.0 * hr / p) * grids[d] for d in range(dim)], axis=-1)
+                    kv = kernel(z.reshape(-1, dim), np.zeros((1, dim)))[:, 0].reshape((ts,) * dim)
+                    blocks.append(np.fft.fftn(kv.astype(np.complex128)))
+                else:
+                    xr = _grid_at(np.zeros(dim), hr, xi, dim)
+                    yt = _grid_at(-dc, ht, xi, dim)
+                    blocks.append(kernel(xr, yt).astype(dtype))
+            canon_of.append(cache[ck])
+            if couplings == "toeplitz":
+                rowperms.append(toeplitz_permutation(2 * p - 1, dim, prm, sg))
+                colperms.append(None)
+            else:
+                gp = grid_permutation(p, dim, prm, sg)
+                rowperms.append(gp)
+                colperms.append(gp)
+    for u in range(ukeys.shape[0] if not symmetry else 0):
         r, t = int(far[first[u], 0]), int(far[first[u], 1])
         if couplings == "toeplitz":
             if test.level[r] != trial.level[t]:
@@ -197,8 +296,19 @@ def interpolation_core(tree: Tree, kernel, p: int, *, nodes: str = "chebyshev",
                   transfer_kind=transfers, coupling_kind=couplings, couplings=blocks,
                   pair_coupling=inv.reshape(-1).astype(np.int64), precision=precision,
                   alpha=alpha, conj_leaf_adjoint=(field == "complex"))
+    if symmetry:
+        core.coupling_canon = np.asarray(canon_of, np.int64)
+        core.coupling_rowperm = rowperms
+        core.coupling_colperm = colperms
     core.kernel = kernel
-    if near == "host":
+    if near == "free":
+        if kernel is laplace:
+            core.set_near_kernel("laplace")
+        elif getattr(kernel, "wavenumber", None) is not None:
+            core.set_near_kernel("helmholtz", kernel.wavenumber)
+        else:
+            raise ValueError("matrix-free near field: laplace or helmholtz kernels only")
+    elif near == "host":
         core.set_near_blocks(near_blocks_from_kernel(trial, plans, kernel, dtype, test=test))
     return core
 

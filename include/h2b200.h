@@ -57,6 +57,15 @@ typedef int h2b_status;
 #define H2B_COUPLING_DIAGONAL 1
 #define H2B_COUPLING_TOEPLITZ 2
 
+/* Near-field storage. H2Factory accepts any matrix-like near operator with the required `mul!`
+ * methods (docs/src/near/storage.md:7-14); besides stored dense blocks the library offers point
+ * kernels whose entries are computed on the fly from the dof coordinates (no near storage):
+ *   LAPLACE    K(x, y) = 1 / (4 pi |x - y|),            0 where x == y;
+ *   HELMHOLTZ  K(x, y) = exp(i k |x - y|) / (4 pi |x - y|), 0 where x == y (complex field). */
+#define H2B_NEAR_STORED 0
+#define H2B_NEAR_LAPLACE 1
+#define H2B_NEAR_HELMHOLTZ 2
+
 /*
  * One tree side (test = rows / y, trial = columns / x) with the plans that use it.
  *
@@ -161,6 +170,30 @@ typedef struct h2b_map_desc {
     const double *near;               /* field scalars; host memory unless near_on_device */
     int64_t near_len;                 /* in field scalars */
     int32_t near_on_device;           /* 1: `near` is a device pointer on the core's device */
+
+    /* ---- matrix-free near field (near_kind != H2B_NEAR_STORED): the block structure above
+     * (near_nrows, near_row, near_ptr, near_col) still names the near leaf pairs, but `near`,
+     * `near_offset` are ignored; entry (i, j) of a block is K(test_points[i], trial_points[j]) for
+     * dof ids i, j, with K the kernel of near_kind. Points are host arrays of xyz triples (unused
+     * coordinates 0). */
+    int32_t near_kind;                /* H2B_NEAR_STORED / H2B_NEAR_LAPLACE / H2B_NEAR_HELMHOLTZ */
+    double near_wavenumber;           /* k of the Helmholtz kernel */
+    const double *test_points;        /* [test.ndofs * 3] */
+    const double *trial_points;       /* [trial.ndofs * 3] */
+
+    /* ---- symmetry-reduced couplings (SymmetryReducedDenseTranslation / PermutedTranslation,
+     * src/farinteractions/i2otranslations/symmetryreduceddense.jl:1-60,
+     * symmetryreducedcollection.jl:1-40, :150-195): the couplings of one symmetry orbit point at
+     * the same canonical data (equal coupling_offset) and read it through 0-based permutations
+     * held in coupling_perm:
+     *   dense:    t[rowperm[i], colperm[j]] = canonical[i, j];
+     *   Toeplitz: t[j] = canonical[rowperm[j]], j the linear index of the padded tensor.
+     * coupling_rowperm / coupling_colperm hold each coupling's permutation offset, -1 for the
+     * identity; NULL when no coupling is permuted (colperm is unused for Toeplitz). */
+    const int64_t *coupling_rowperm;  /* [ncouplings] */
+    const int64_t *coupling_colperm;  /* [ncouplings] */
+    const int32_t *coupling_perm;
+    int64_t coupling_perm_len;
 } h2b_map_desc;
 
 typedef struct h2b_core h2b_core;

@@ -342,15 +342,39 @@ static int SFX(farmul)(const h2b_map_desc *d, int mode, int nrhs, const SC *x, i
                 const int src = ds->i2o_src[p];
                 const int slvl = as->level[src];
                 const int64_t snc = SFX(ncoef)(as, slvl);
-                const int64_t coff = d->coupling_offset[ds->i2o_coupling[p]];
+                const int64_t key = ds->i2o_coupling[p];
+                const int64_t coff = d->coupling_offset[key];
+                /* symmetry-reduced couplings: canonical data read through permutations */
+                const int32_t *rp = (d->coupling_rowperm && d->coupling_rowperm[key] >= 0)
+                                        ? d->coupling_perm + d->coupling_rowperm[key] : NULL;
+                const int32_t *cp = (d->coupling_colperm && d->coupling_colperm[key] >= 0)
+                                        ? d->coupling_perm + d->coupling_colperm[key] : NULL;
                 if (d->coupling_kind == H2B_COUPLING_DENSE) {
                     /* mul!(out, op(block), in[, true, true]), i2otranslationcollection.jl:367-409.
                        The stored block of the resolved key is ncoef(key recv) x ncoef(key transl). */
                     const SC *B = (const SC *)(d->coupling + coff);
                     const int64_t ldb = (i2oop == 0) ? nc : snc;
-                    for (int q = 0; q < d->ncomp * nrhs; ++q)
-                        SFX(dense_apply)(B, ldb, nc, snc, i2oop, am.m + am.off[src] + q * snc,
-                                         out + q * nc, initialized);
+                    for (int q = 0; q < d->ncomp * nrhs; ++q) {
+                        const SC *in = am.m + am.off[src] + q * snc;
+                        SC *o = out + q * nc;
+                        if (!rp && !cp) {
+                            SFX(dense_apply)(B, ldb, nc, snc, i2oop, in, o, initialized);
+                            continue;
+                        }
+                        /* PermutedDenseTranslation: gather the input, multiply by the canonical
+                           block, scatter the output; transposed maps gather with the row and
+                           scatter with the column permutation (symmetryreduceddense.jl:84-95) */
+                        const int32_t *gp = (i2oop == 0) ? cp : rp, *sp = (i2oop == 0) ? rp : cp;
+                        SC *w = (SC *)malloc(sizeof(SC) * (size_t)(snc + nc));
+                        SC *yv = w + snc;
+                        for (int64_t j = 0; j < snc; ++j) w[j] = in[gp ? gp[j] : j];
+                        SFX(dense_apply)(B, ldb, nc, snc, i2oop, w, yv, 0);
+                        for (int64_t i = 0; i < nc; ++i) {
+                            const int64_t k = sp ? sp[i] : i;
+                            o[k] = initialized ? o[k] + yv[i] : yv[i];
+                        }
+                        free(w);
+                    }
                 } else if (d->coupling_kind == H2B_COUPLING_DIAGONAL) {
                     /* elementwisemul!, adjoint conjugates (i2otranslationcollection.jl:415-495) */
                     const SC *D = (const SC *)(d->coupling + coff);
@@ -367,7 +391,9 @@ static int SFX(farmul)(const h2b_map_desc *d, int mode, int nrhs, const SC *x, i
                     const double _Complex *tin = am.t + am.toff[src];
                     for (int q = 0; q < d->ncomp * nrhs; ++q)
                         for (int64_t e = 0; e < nt; ++e) {
-                            const double _Complex kv = (i2oop == 2) ? conj(K[e]) : K[e];
+                            /* PermutedTranslation: t[e] = canonical[perm[e]] */
+                            const double _Complex ke = K[rp ? rp[e] : e];
+                            const double _Complex kv = (i2oop == 2) ? conj(ke) : ke;
                             const double _Complex v = kv * tin[q * nt + e];
                             tout[q * nt + e] = initialized ? tout[q * nt + e] + v : v;
                         }

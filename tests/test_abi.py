@@ -50,6 +50,11 @@ def test_struct_layout_matches_header():
     names = re.findall(r"\*?(\w+);", side)
     fields = [f for f, _ in _abi.SideDesc._fields_]
     assert [n for n in names if n in fields] == fields
+    mapd = txt[txt.index("typedef struct h2b_map_desc"):txt.index("} h2b_map_desc;")]
+    mapd = re.sub(r"/\*.*?\*/", "", mapd, flags=re.S)
+    names = re.findall(r"\b(\w+)(?:\[[^\]]*\])*;", mapd)
+    fields = [f for f, _ in _abi.MapDesc._fields_]
+    assert [n for n in names if n in fields] == fields
 
 
 @pytest.fixture
@@ -78,6 +83,9 @@ def create(lib, desc):
     (lambda d, k: k.bad_near(d), "near block"),
     (lambda d, k: k.bad_stage_order(d), "aggregation"),
     (lambda d, k: k.bad_parent(d), "parent"),
+    (lambda d, k: setattr(d, "near_kind", 7), "near kind"),
+    (lambda d, k: setattr(d, "near_kind", _abi.H2B_NEAR_LAPLACE), "without points"),
+    (lambda d, k: k.helmholtz_on_real(d), "Helmholtz near kernel on a real map"),
 ])
 def test_malformed_maps_are_rejected(lib, small_core, mutate, msg):
     desc, keep = flatten(small_core)
@@ -110,11 +118,37 @@ def test_malformed_maps_are_rejected(lib, small_core, mutate, msg):
             arr = np.ctypeslib.as_array(d.test.parent, shape=(d.test.nnodes,))
             arr[5] = d.test.nnodes + 3
 
+        @staticmethod
+        def helmholtz_on_real(d):
+            pts = np.zeros(3 * max(d.test.ndofs, d.trial.ndofs))
+            keep.append(pts)
+            d.test_points = d.trial_points = pts.ctypes.data_as(C.POINTER(C.c_double))
+            d.near_kind = _abi.H2B_NEAR_HELMHOLTZ
+
     mutate(desc, K)
     st, err = create(lib, desc)
     assert st == _abi.H2B_ERR_INVALID
     assert msg in err
     del keep
+
+
+def test_bad_permutations_are_rejected(lib):
+    rng = np.random.default_rng(2)
+    t = build_tree(rng.random((800, 3)), maxvalues=16, root_center=[0.5] * 3, root_halfsize=0.5)
+    core = methods.interpolation_core(t, methods.laplace, 2, symmetry=True)
+    for how, msg in (("dup", "not a permutation"), ("range", "not a permutation"), ("off", "out of range")):
+        desc, keep = flatten(core)
+        arr = np.ctypeslib.as_array(desc.coupling_perm, shape=(desc.coupling_perm_len,))
+        offs = np.ctypeslib.as_array(desc.coupling_rowperm, shape=(desc.ncouplings,))
+        if how == "dup":
+            arr[1] = arr[0]
+        elif how == "range":
+            arr[0] = 99
+        else:
+            offs[offs >= 0] = desc.coupling_perm_len
+        st, err = create(lib, desc)
+        assert st == _abi.H2B_ERR_INVALID and msg in err, (how, err)
+        del keep
 
 
 def test_bad_call_arguments_without_device(lib):

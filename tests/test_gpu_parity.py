@@ -122,6 +122,18 @@ CASES = {
     # so the per-node Toeplitz kernel runs
     "toeplitz-laplace-unshared": lambda: _unshared(methods.interpolation_core(
         _cube(2000, 5, depth=3), methods.laplace, 4, nodes="equispaced", couplings="toeplitz")),
+    # symmetry-reduced couplings: one canonical block / spectrum per orbit of the cube's signed
+    # axis permutations, read through permutations
+    "sym-cheb-laplace": lambda: methods.interpolation_core(_cube(3000, 1, maxvalues=40), methods.laplace, 4,
+                                                           symmetry=True),
+    "sym-cheb-helmholtz": lambda: methods.interpolation_core(_cube(2500, 2, maxvalues=48), methods.helmholtz(4.0),
+                                                             3, symmetry=True),
+    "sym-toeplitz-laplace": lambda: methods.interpolation_core(_cube(4000, 3, depth=4), methods.laplace, 4,
+                                                               nodes="equispaced", couplings="toeplitz",
+                                                               symmetry=True),
+    "sym-toeplitz-helmholtz": lambda: methods.interpolation_core(_cube(3000, 4, depth=4), methods.helmholtz(3.0), 3,
+                                                                 nodes="equispaced", couplings="toeplitz",
+                                                                 transfers="separable", symmetry=True),
     # Petrov (rectangular) maps: test and trial trees on different point sets and depths
     "petrov-cheb-laplace": lambda: methods.interpolation_core(
         _cube(3000, 6, maxvalues=40), methods.laplace, 4, trial=_cube(1100, 7, maxvalues=30)),

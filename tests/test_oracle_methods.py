@@ -150,3 +150,26 @@ def test_petrov_interpolation_vs_dense():
         x = rng.standard_normal(op.shape[1]) + 1j * rng.standard_normal(op.shape[1])
         y = oracle.matvec(core, x, mode)
         assert np.linalg.norm(y - op @ x) / np.linalg.norm(op @ x) < 5e-3
+
+
+@pytest.mark.parametrize("kind", ["dense", "toeplitz"])
+def test_symmetry_reduced_couplings_equal_unreduced(kind):
+    """symmetryreduceddense.jl / symmetryreducedcollection.jl, test_toeplitz3d.jl:120-140: one
+    stored coupling per orbit of the cube's signed axis permutations (about 20x fewer), read
+    through permutations, gives the map of one coupling per translation, in every orientation."""
+    rng = np.random.default_rng(7)
+    if kind == "dense":
+        tree = build_tree(rng.random((2000, 3)), maxvalues=40, root_center=[0.5] * 3, root_halfsize=0.5)
+        mk = lambda sym: methods.interpolation_core(tree, methods.helmholtz(3.0), 3, symmetry=sym)
+    else:
+        tree = build_tree(rng.random((3000, 3)), depth=4, root_center=[0.5] * 3, root_halfsize=0.5)
+        mk = lambda sym: methods.interpolation_core(tree, methods.laplace, 4, nodes="equispaced",
+                                                    couplings="toeplitz", symmetry=sym)
+    plain, reduced = mk(False), mk(True)
+    assert len(plain.couplings) / len(reduced.couplings) > 5
+    for mode in range(3):
+        x = rng.standard_normal(tree.npoints) + 1j * rng.standard_normal(tree.npoints)
+        if plain.field == "real":
+            x = x.real
+        a, b = oracle.matvec(plain, x, mode), oracle.matvec(reduced, x, mode)
+        assert rel(b, a) < 1e-13
