@@ -75,7 +75,8 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 EXPORTS = [
     "h2b_version", "h2b_last_error", "h2b_core_create", "h2b_core_destroy", "h2b_core_get_info",
     "h2b_workspace_create", "h2b_workspace_destroy", "h2b_matvec", "h2b_matvec_host",
-    "h2b_farmul", "h2b_nearmul", "h2b_farmul_noalloc",
+    "h2b_farmul", "h2b_nearmul", "h2b_farmul_noalloc", "h2b_map_blob_write", "h2b_map_blob_read",
+    "h2b_core_create_from_blob",
 ]
 
 H2B_NOALLOC_SCRATCH_BYTES = 16 << 20
@@ -114,6 +115,9 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.h2b_core_create.argtypes = [C.POINTER(MapDesc), C.c_int32, C.POINTER(vp)]
     lib.h2b_core_destroy.argtypes = [vp]
     lib.h2b_core_get_info.argtypes = [vp, C.POINTER(CoreInfo)]
+    lib.h2b_map_blob_write.argtypes = [C.POINTER(MapDesc), vp, C.c_size_t, C.POINTER(C.c_size_t)]
+    lib.h2b_map_blob_read.argtypes = [vp, C.c_size_t, C.POINTER(MapDesc)]
+    lib.h2b_core_create_from_blob.argtypes = [vp, C.c_size_t, C.c_int32, C.POINTER(vp)]
     lib.h2b_workspace_create.argtypes = [vp, C.c_int32, C.POINTER(vp)]
     lib.h2b_workspace_destroy.argtypes = [vp]
     mv = [vp, C.c_int32, C.c_int32, vp, C.c_int64, vp, C.c_int64, _f64p, _f64p, vp]

@@ -14,6 +14,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from dataclasses import dataclass, field
 
@@ -291,6 +292,65 @@ def flatten(core: H2Core):
 # Device objects
 # ---------------------------------------------------------------------------------------------
 
+@dataclass
+class MapShape:
+    """What a workspace needs of a core that was loaded from a map blob (no host-side H2Core)."""
+
+    field: str
+    size: tuple
+    precision: str
+
+    @property
+    def dtype(self):
+        return np.complex128 if self.field == "complex" else np.float64
+
+
+def _aligned(nbytes: int) -> np.ndarray:
+    """An 8-byte aligned uint8 buffer (the blob format's alignment)."""
+    return np.zeros((nbytes + 7) // 8, np.uint64).view(np.uint8)[:nbytes]
+
+
+def map_blob(core: H2Core) -> np.ndarray:
+    """The core as one self-contained byte image (h2b_map_blob_write); near blocks held on the
+    device are copied to the host first."""
+    import copy
+
+    if core.near_device is not None:
+        c = copy.copy(core)
+        c.near_data, c.near_device = core.near_device.cpu().numpy(), None
+        core = c
+    lib = _abi.load_library()
+    desc, keep = flatten(core)
+    size = C.c_size_t()
+    _abi.check(lib.h2b_map_blob_write(C.byref(desc), None, 0, C.byref(size)))
+    buf = _aligned(size.value)
+    _abi.check(lib.h2b_map_blob_write(C.byref(desc), buf.ctypes.data_as(C.c_void_p), size.value, C.byref(size)))
+    del keep
+    return buf
+
+
+def save_map(core: H2Core, path: str) -> int:
+    """Write the map blob of `core` to `path`; returns its size in bytes."""
+    buf = map_blob(core)
+    with open(path, "wb") as f:
+        f.write(buf.tobytes())
+    return buf.size
+
+
+def read_blob(blob) -> tuple:
+    """(aligned buffer, h2b_map_desc pointing into it) of a blob given as bytes, array or path."""
+    if isinstance(blob, (str, os.PathLike)):
+        with open(blob, "rb") as f:
+            data = f.read()
+    else:
+        data = bytes(np.asarray(blob, np.uint8).tobytes()) if not isinstance(blob, bytes) else blob
+    buf = _aligned(len(data))
+    buf[:] = np.frombuffer(data, np.uint8)
+    desc = _abi.MapDesc()
+    _abi.check(_abi.load_library().h2b_map_blob_read(buf.ctypes.data_as(C.c_void_p), buf.size, C.byref(desc)))
+    return buf, desc
+
+
 class DeviceCore:
     """The read-only core in HBM (h2b_core)."""
 
@@ -303,6 +363,22 @@ class DeviceCore:
         _abi.check(self.lib.h2b_core_create(C.byref(desc), device, C.byref(h)))
         self.handle = h
         del keep
+
+    @classmethod
+    def from_blob(cls, blob, device: int = 0) -> "DeviceCore":
+        """A core built straight from a map blob (bytes, uint8 array or file path)."""
+        buf, desc = read_blob(blob)
+        self = cls.__new__(cls)
+        self.lib = _abi.load_library()
+        self.device = device
+        self.core = MapShape("complex" if desc.field == _abi.H2B_COMPLEX else "real",
+                             (desc.test.ndofs, desc.trial.ndofs),
+                             "fp32" if desc.precision == _abi.H2B_FP32 else "fp64")
+        h = C.c_void_p()
+        _abi.check(self.lib.h2b_core_create_from_blob(buf.ctypes.data_as(C.c_void_p), buf.size, device,
+                                                       C.byref(h)))
+        self.handle = h
+        return self
 
     def info(self) -> _abi.CoreInfo:
         out = _abi.CoreInfo()

@@ -35,6 +35,15 @@ h2b_status fail(h2b_status st, const char *fmt, ...) {
     return st;
 }
 
+}  // namespace
+
+h2b_status h2b::set_error_text(h2b_status st, const char *msg) {
+    g_err = msg;
+    return st;
+}
+
+namespace {
+
 #define CUDA_TRY(expr)                                                                         \
     do {                                                                                       \
         cudaError_t e_ = (expr);                                                               \

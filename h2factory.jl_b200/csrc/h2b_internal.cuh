@@ -130,6 +130,9 @@ struct DNear {
 };
 
 // Sibling groups for the Toeplitz I2O (i2o_sibling_kernel): the receiving children of one parent.
+// Record `msg` as the calling thread's error text (h2b_last_error) and return `st`.
+h2b_status set_error_text(h2b_status st, const char *msg);
+
 struct SibGroups {
     int ngroups = 0;
     const int *recv = nullptr;         // [ngroups*8] receiving node per child slot, -1 if none

@@ -212,7 +212,7 @@ near_rows_mma_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const dou
                      int64_t ldx, double *__restrict__ y, int64_t ldy, double alpha, double beta,
                      bool beta_zero) {
     constexpr int R = 8 * NT;
-    constexpr int XS = R + 4;  // padded row of the x chunk: conflict-free fragment reads
+    constexpr int XS = R + 4;  // padded row of the x chunk
     constexpr int RPP = 64;
     extern __shared__ unsigned char smem_raw[];
     const int g = blockIdx.x;

@@ -129,7 +129,7 @@ typedef struct h2b_side_desc {
      * column-major, axis 1 first (src/maps/leveltranslator.jl:168-265). */
     const int64_t *transfer_offset; /* [(nlevels+1)*nsectors], -1 where absent */
     const double *transfer;
-    int64_t transfer_len;
+    int64_t transfer_len;        /* in field scalars */
 } h2b_side_desc;
 
 /* A complete map (H2Factory's core + the flattened plans that a workspace schedules). */
@@ -221,6 +221,18 @@ const char *h2b_last_error(void);
 h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **out);
 h2b_status h2b_core_destroy(h2b_core *core);
 h2b_status h2b_core_get_info(const h2b_core *core, h2b_core_info *out);
+
+/* ---- map blob: a descriptor as one self-contained, 8-byte aligned byte image, to store a core
+ * on disk and load it in another process. The reference keeps its cores inside a Julia session and
+ * has no file format; the blob carries the core's read-only data (src/maps/core.jl:1-60) and the
+ * plans a workspace is built from (src/maps/workspace.jl:81-100).
+ *   h2b_map_blob_write: buf = NULL returns the size in *size; near blocks must be host memory.
+ *   h2b_map_blob_read: fills *out with pointers INTO `blob` (keep it alive while *out is used);
+ *     checks the layout and every array length, not the contents (h2b_core_create does that).
+ *   h2b_core_create_from_blob: read + h2b_core_create. */
+h2b_status h2b_map_blob_write(const h2b_map_desc *desc, void *buf, size_t cap, size_t *size);
+h2b_status h2b_map_blob_read(const void *blob, size_t bytes, h2b_map_desc *out);
+h2b_status h2b_core_create_from_blob(const void *blob, size_t bytes, int32_t device, h2b_core **out);
 
 /* Mutable per-request state (moments, spectra, host staging) for up to `max_nrhs` right-hand
  * sides: H2Workspace(core) / similarworkspace (src/maps/workspace.jl:81-113). Several

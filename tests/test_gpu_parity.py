@@ -134,6 +134,9 @@ CASES = {
     "sym-toeplitz-helmholtz": lambda: methods.interpolation_core(_cube(3000, 4, depth=4), methods.helmholtz(3.0), 3,
                                                                  nodes="equispaced", couplings="toeplitz",
                                                                  transfers="separable", symmetry=True),
+    # sphere, Chebyshev p = 6 (216 coefficients), Helmholtz, leaves <= 128 points, symmetry-reduced
+    "sphere-cheb6-helmholtz-sym": lambda: methods.interpolation_core(
+        _sphere(12000, 10, maxvalues=128), methods.helmholtz(8 * np.pi * 0.45), 6, symmetry=True),
     # Petrov (rectangular) maps: test and trial trees on different point sets and depths
     "petrov-cheb-laplace": lambda: methods.interpolation_core(
         _cube(3000, 6, maxvalues=40), methods.laplace, 4, trial=_cube(1100, 7, maxvalues=30)),
@@ -141,6 +144,17 @@ CASES = {
         _cube(2500, 8, depth=4), methods.helmholtz(3.0), 3, nodes="equispaced", couplings="toeplitz",
         trial=_cube(4000, 9, depth=4)),
 }
+
+
+def _sphere(n, seed, **kw):
+    """Fibonacci sphere (radius 0.45 in the unit cube) with jitter 0.1 x the point spacing: the
+    geometry of the 1M-point Helmholtz configuration, at a size the oracle checks in seconds."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n) + 0.5
+    phi, th = np.arccos(1 - 2 * i / n), np.pi * (1 + 5 ** 0.5) * i
+    p = np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], axis=1)
+    p = p + 0.1 * np.sqrt(4 * np.pi / n) * rng.standard_normal(p.shape)
+    return build_tree(0.5 + 0.45 * p, root_center=[0.5] * 3, root_halfsize=0.5, **kw)
 
 
 def _unshared(core):
@@ -280,3 +294,15 @@ def test_c1_config_full_size():
     assert rel(got, oracle.matvec(core, x)) < TOL64
     K = methods.kernel_matrix(methods.laplace, pts, pts)
     assert rel(got, K @ x) < 5e-3
+
+
+def test_sphere_helmholtz_32_rhs():
+    """32 complex right-hand sides per product, forward and adjoint (the sphere configuration's
+    block size), against the oracle."""
+    core = CASES["sphere-cheb6-helmholtz-sym"]()
+    ws = h2.H2Workspace(core, max_nrhs=32)
+    desc = h2.flatten(core)
+    for mode, op in (ORIENT[0], ORIENT[2]):
+        x = _x(core, 32, 17, mode)
+        want = oracle.matvec(core, x, mode, desc=desc)
+        assert rel(run(h2.mul_, op(ws), x), want) < TOL64, mode
