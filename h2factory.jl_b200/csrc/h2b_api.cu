@@ -140,6 +140,7 @@ struct h2b_workspace {
     int max_nrhs = 1;
     void *am = nullptr, *dm = nullptr, *as = nullptr, *ds = nullptr;
     void *xbuf = nullptr, *ybuf = nullptr;  // staging for h2b_matvec_host
+    void *xnear = nullptr;  // gathered x rows for the tensor-core near kernel (real, >= 8 RHS)
     std::atomic<int> busy{0};
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr;
@@ -554,6 +555,7 @@ h2b_status build_side(h2b_core *c, const h2b_map_desc &d, const h2b_side_desc &s
     D.nnodes = s.nnodes;
     D.nlevels = s.nlevels;
     D.ndofs = s.ndofs;
+    D.nvalues = s.value_ptr[s.nnodes];
     int *p;
     CUDA_TRY(c->upload(&p, s.level, s.nnodes)); D.level = p;
     CUDA_TRY(c->upload(&p, s.parent, s.nnodes)); D.parent = p;
@@ -1077,6 +1079,8 @@ h2b_status h2b_workspace_create(h2b_core *core, int32_t max_nrhs, h2b_workspace 
     if (e == cudaSuccess) e = al(&ws->ds, spec * ssz);
     if (e == cudaSuccess) e = al(&ws->xbuf, ndof * vsz);
     if (e == cudaSuccess) e = al(&ws->ybuf, ndof * vsz);
+    if (e == cudaSuccess && !cplx && max_nrhs >= 8)
+        e = al(&ws->xnear, (size_t)std::max(core->test.ndofs, core->trial.ndofs) * 16 * sizeof(double));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ws->aux, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming);
@@ -1190,7 +1194,7 @@ h2b_status run(h2b_workspace *ws, Kind kind, int32_t mode, int32_t nrhs, const v
     const SideHost &cols = c->trial;
     h2b_status s = H2B_OK;
     if (kind == KIND_NEAR) {
-        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b, st));
+        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b, ws->xnear, st));
     } else if (kind == KIND_FAR) {
         if (!alpha) {
             CUDA_TRY(launch_zero_columns(cplx, nrhs, nout, y, ldy, st));
@@ -1202,7 +1206,7 @@ h2b_status run(h2b_workspace *ws, Kind kind, int32_t mode, int32_t nrhs, const v
         // near on the auxiliary stream, far on the caller's; the leaf scatter waits for the near
         CUDA_TRY(cudaEventRecord(ws->ev_fork, st));
         CUDA_TRY(cudaStreamWaitEvent(ws->aux, ws->ev_fork, 0));
-        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b, ws->aux));
+        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b, ws->xnear, ws->aux));
         CUDA_TRY(cudaEventRecord(ws->ev_join, ws->aux));
         s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(aA, a), cdouble{1.0, 0.0}, st, ws->ev_join);
     }

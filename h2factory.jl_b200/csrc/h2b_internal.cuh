@@ -80,6 +80,7 @@ __host__ __device__ __forceinline__ void from_cx(cdouble s, cfloat &out) { out =
 // ---------------------------------------------------------------------------------------------
 struct DSide {
     int nnodes, nlevels, ndofs;
+    int nvalues;             // value_ptr[nnodes]: dof entries held by the leaves
     const int *level, *parent, *sector, *child_ptr, *child, *value_ptr, *value;
     const int *shape;        // [(nlevels+1)*3]
     const int64_t *mom_off;  // [nnodes] moment offset per unit right-hand side (elements of T)
@@ -182,7 +183,7 @@ cudaError_t launch_leaf_disaggregate(bool cplx, int precision, const DMap &m, co
                                      cudaStream_t st);
 cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &test, const DSide &trial,
                         int nrhs, const void *x, int64_t ldx, void *y, int64_t ldy, cdouble alpha,
-                        cdouble beta, cudaStream_t st);
+                        cdouble beta, void *xp, cudaStream_t st);
 int64_t near_padded_ld(bool cplx, int n);
 cudaError_t launch_near_repack(bool cplx, const void *src, const int64_t *src_off, const int *blk_row,
                                const int *blk_col, const DSide &rows, const DSide &cols, void *dst,

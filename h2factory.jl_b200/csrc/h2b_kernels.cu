@@ -83,6 +83,98 @@ __device__ __forceinline__ void tile_gemm_l(bool kfast, int m0, int mt, int kk, 
     }
 }
 
+// The same tile product on the FP64 tensor cores (mma.sync m8n8k4 .f64): warp w owns output rows
+// 8w..8w+7 of the tile (TG_M = 64 rows for 8 warps) and both 8-wide right-hand-side halves of
+// TG_Q. Complex tiles take four real products per k-step (re = ar br - ai bi, im = ar bi + ai br).
+// Fragment layout (PTX ISA, m8n8k4 .f64): A[lane/4][lane%4], B[lane%4][lane/4],
+// C[lane/4][2*(lane%4) + i]. Rows past mt and columns past nq compute on stale shared memory and
+// are never stored; k past the chunk is zero-filled, as in tile_gemm_l.
+__device__ __forceinline__ void dmma8(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+template <class A> struct MmaAcc;
+template <> struct MmaAcc<double> {
+    double c[2][2];
+    __device__ void zero() { c[0][0] = c[0][1] = c[1][0] = c[1][1] = 0.0; }
+    __device__ void step(double a, const double (&b)[2]) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) dmma8(c[u], a, b[u]);
+    }
+    __device__ double get(int u, int h) const { return c[u][h]; }
+};
+template <> struct MmaAcc<cdouble> {
+    double re[2][2], im[2][2];
+    __device__ void zero() {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) re[u][0] = re[u][1] = im[u][0] = im[u][1] = 0.0;
+    }
+    __device__ void step(cdouble a, const cdouble (&b)[2]) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            dmma8(re[u], a.x, b[u].x);
+            dmma8(re[u], -a.y, b[u].y);
+            dmma8(im[u], a.x, b[u].y);
+            dmma8(im[u], a.y, b[u].x);
+        }
+    }
+    __device__ cdouble get(int u, int h) const { return {re[u][h], im[u][h]}; }
+};
+
+template <class A, class MLoad, class XLoad>
+__device__ __forceinline__ void tile_gemm_mma_l(bool kfast, int m0, int mt, int kk, int nq, MLoad mload,
+                                                XLoad xload, A *Ms, A *Xs, MmaAcc<A> &acc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g4 = lane >> 2, t4 = lane & 3;
+    for (int k0 = 0; k0 < kk; k0 += TG_K) {
+        const int kc = min(TG_K, kk - k0);
+        __syncthreads();
+        if (kfast) {
+            for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
+                const int k = idx % TG_K, i = idx / TG_K;
+                Ms[i * TG_LD + k] = k < kc ? mload(m0 + i, k0 + k) : A{};
+            }
+        } else {
+            for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
+                const int i = idx % mt, k = idx / mt;
+                Ms[i * TG_LD + k] = k < kc ? mload(m0 + i, k0 + k) : A{};
+            }
+        }
+        for (int idx = threadIdx.x; idx < TG_K * nq; idx += blockDim.x) {
+            const int k = idx % TG_K, q = idx / TG_K;
+            Xs[k * TG_Q + q] = k < kc ? xload(k0 + k, q) : A{};
+        }
+        __syncthreads();
+        if (8 * warp < mt) {
+            const A *mrow = Ms + (8 * warp + g4) * TG_LD + t4;
+            const A *xcol = Xs + t4 * TG_Q + g4;
+#pragma unroll
+            for (int k = 0; k < TG_K; k += 4) {
+                const A a = mrow[k];
+                const A b[2] = {xcol[k * TG_Q], xcol[k * TG_Q + 8]};
+                acc.step(a, b);
+            }
+        }
+    }
+}
+
+// f(i, q, value) for every element of the warp's C fragments inside the mt x nq tile
+template <class A, class F>
+__device__ __forceinline__ void mma_store(const MmaAcc<A> &acc, int mt, int nq, F f) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = 8 * warp + (lane >> 2);
+    if (i >= mt) return;
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int q = 8 * u + 2 * (lane & 3) + h;
+            if (q < nq) f(i, q, acc.get(u, h));
+        }
+}
+
 // op(M)[i, k] = M[i + k*ldm] (trans = false) or M[k + i*ldm] (trans = true), conjugated when cjg.
 template <class T, class A, class XLoad>
 __device__ __forceinline__ void tile_gemm(const T *__restrict__ M, int64_t ldm, bool trans, bool cjg, int m0,
@@ -101,7 +193,7 @@ __device__ __forceinline__ void tile_zero(A (&acc)[TG_O]) {
     for (int j = 0; j < TG_O; ++j) acc[j] = A{};
 }
 
-// smem for tile_gemm: Ms [TG_M][TG_LD] + Xs [TG_K][TG_Q]
+// smem for tile_gemm and tile_gemm_mma_l: Ms [TG_M][TG_LD] + Xs [TG_K][TG_Q]
 template <class A>
 constexpr size_t tile_smem() { return (size_t)(TG_M * TG_LD + TG_K * TG_Q) * sizeof(A); }
 
@@ -109,7 +201,7 @@ constexpr size_t tile_smem() { return (size_t)(TG_M * TG_LD + TG_K * TG_Q) * siz
 // A1: m_leaf[c][r] = op(C_c) x[values]   (op = conj for adjoint maps with conjugating leaves);
 // RCH right-hand sides share each pass over the collection
 // ---------------------------------------------------------------------------------------------
-template <class T, class V>
+template <class T, class V, bool MMA>
 __global__ void __launch_bounds__(256)
 leaf_aggregate_kernel(DMap m, DSide s, const int *__restrict__ leaves, bool conjc, int nrhs,
                       const V *__restrict__ x, int64_t ldx, T *__restrict__ am) {
@@ -126,16 +218,29 @@ leaf_aggregate_kernel(DMap m, DSide s, const int *__restrict__ leaves, bool conj
             const int nq = min(TG_Q, nrhs - q0);
             for (int m0 = 0; m0 < nc; m0 += TG_M) {
                 const int mt = min(TG_M, nc - m0);
-                A acc[TG_O];
-                tile_zero(acc);
-                tile_gemm(C + (int64_t)c * nc * nv, nc, false, conjc, m0, mt, nv, nq,
-                          [&](int k, int q) -> A { return x[(int64_t)(q0 + q) * ldx + s.value[v0 + k]]; },
-                          Ms, Xs, acc);
+                const T *Cc = C + (int64_t)c * nc * nv;
+                if constexpr (!MMA) {  // one right-hand side: FMA tile (an MMA would idle 7 of 8 columns)
+                    A acc[TG_O];
+                    tile_zero(acc);
+                    tile_gemm(Cc, nc, false, conjc, m0, mt, nv, nq,
+                              [&](int k, int q) -> A { return x[(int64_t)(q0 + q) * ldx + s.value[v0 + k]]; },
+                              Ms, Xs, acc);
 #pragma unroll
-                for (int j = 0; j < TG_O; ++j) {
-                    const int o = threadIdx.x + j * blockDim.x;
-                    if (o < mt * nq)
-                        narrow(acc[j], mom[((int64_t)c * nrhs + q0 + o / mt) * nc + m0 + o % mt]);
+                    for (int j = 0; j < TG_O; ++j) {
+                        const int o = threadIdx.x + j * blockDim.x;
+                        if (o < mt * nq)
+                            narrow(acc[j], mom[((int64_t)c * nrhs + q0 + o / mt) * nc + m0 + o % mt]);
+                    }
+                } else {
+                MmaAcc<A> acc;  // FP64 tensor cores (256 threads: 8 warps x 8 rows)
+                acc.zero();
+                tile_gemm_mma_l(false, m0, mt, nv, nq,
+                                [&](int i, int k) -> A { return wide(cj(Cc[i + (int64_t)k * nc], conjc)); },
+                                [&](int k, int q) -> A { return x[(int64_t)(q0 + q) * ldx + s.value[v0 + k]]; },
+                                Ms, Xs, acc);
+                mma_store(acc, mt, nq, [&](int i, int q, A v) {
+                    narrow(v, mom[((int64_t)c * nrhs + q0 + q) * nc + m0 + i]);
+                });
                 }
             }
         }
@@ -193,7 +298,7 @@ __device__ void separable_block(const T *M, const int *sp, const int *sc, int di
 // ---------------------------------------------------------------------------------------------
 // A2: m_p = sum over children of op(T_{level(c), sector(c)}) m_c, first child overwriting.
 // ---------------------------------------------------------------------------------------------
-template <class T>
+template <class T, bool MMA>
 __global__ void transfer_up_kernel(DMap m, DSide s, const int *__restrict__ nodes, bool conjt,
                                    int nrhs, T *__restrict__ am) {
     using A = typename ScalarTraits<T>::Acc;
@@ -243,20 +348,35 @@ __global__ void transfer_up_kernel(DMap m, DSide s, const int *__restrict__ node
             const int nqc = min(TG_Q, nq - q0);
             for (int m0 = 0; m0 < nout; m0 += TG_M) {
                 const int mt = min(TG_M, nout - m0);
-                A acc[TG_O];
-                tile_zero(acc);
-                for (int k = c0; k < c1; ++k) {
-                    const int ch = s.child[k];
-                    const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
-                    const T *mc = am + s.mom_off[ch] * nrhs;
-                    tile_gemm(Tk, nout, false, conjt, m0, mt, nin, nqc,
-                              [&](int kk, int q) -> A { return wide(mc[(int64_t)(q0 + q) * nin + kk]); }, Ms, Xs,
-                              acc);
-                }
+                if constexpr (MMA) {
+                    MmaAcc<A> acc;  // FP64 tensor cores (256 threads: 8 warps x 8 rows)
+                    acc.zero();
+                    for (int k = c0; k < c1; ++k) {
+                        const int ch = s.child[k];
+                        const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
+                        const T *mc = am + s.mom_off[ch] * nrhs;
+                        tile_gemm_mma_l(false, m0, mt, nin, nqc,
+                                        [&](int i, int kk) -> A { return wide(cj(Tk[i + (int64_t)kk * nout], conjt)); },
+                                        [&](int kk, int q) -> A { return wide(mc[(int64_t)(q0 + q) * nin + kk]); },
+                                        Ms, Xs, acc);
+                    }
+                    mma_store(acc, mt, nqc, [&](int i, int q, A v) { narrow(v, mp[(int64_t)(q0 + q) * nout + m0 + i]); });
+                } else {
+                    A acc[TG_O];
+                    tile_zero(acc);
+                    for (int k = c0; k < c1; ++k) {
+                        const int ch = s.child[k];
+                        const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
+                        const T *mc = am + s.mom_off[ch] * nrhs;
+                        tile_gemm(Tk, nout, false, conjt, m0, mt, nin, nqc,
+                                  [&](int kk, int q) -> A { return wide(mc[(int64_t)(q0 + q) * nin + kk]); }, Ms, Xs,
+                                  acc);
+                    }
 #pragma unroll
-                for (int j = 0; j < TG_O; ++j) {
-                    const int o = threadIdx.x + j * blockDim.x;
-                    if (o < mt * nqc) narrow(acc[j], mp[(int64_t)(q0 + o / mt) * nout + m0 + o % mt]);
+                    for (int j = 0; j < TG_O; ++j) {
+                        const int o = threadIdx.x + j * blockDim.x;
+                        if (o < mt * nqc) narrow(acc[j], mp[(int64_t)(q0 + o / mt) * nout + m0 + o % mt]);
+                    }
                 }
             }
         }
@@ -585,7 +705,7 @@ toeplitz_out_cube4_real_kernel(DSide s, const int *__restrict__ nodes, int ntran
 // (src/farinteractions/i2otranslations/i2oprotocol.jl:87-92, i2otranslationcollection.jl:367-495,
 // toeplitzi2ocollection.jl:110-193). The first pair overwrites.
 // ---------------------------------------------------------------------------------------------
-template <class T>
+template <class T, bool MMA>
 __global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mode,
                            int nrhs, const T *__restrict__ am, T *__restrict__ dm,
                            const typename ScalarTraits<T>::Complex *__restrict__ as,
@@ -659,46 +779,57 @@ __global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, cons
             }
         return;
     }
-    // dense: out (nc x nq) = sum over pairs of op(B) X_src, all right-hand sides per pass
+    // dense: out (nc x nq) = sum over pairs of op(B) X_src, all right-hand sides per pass, on
+    // the FP64 tensor cores (tile_gemm_mma_l; the CTA has the 8 warps its tiling needs)
     extern __shared__ unsigned char smem_raw[];
     A *Ms = reinterpret_cast<A *>(smem_raw), *Xs = Ms + TG_M * TG_LD;
     for (int q0 = 0; q0 < nq; q0 += TG_Q) {
         const int nqc = min(TG_Q, nq - q0);
         for (int m0 = 0; m0 < nc; m0 += TG_M) {
             const int mt = min(TG_M, nc - m0);
-            A acc[TG_O];
-            tile_zero(acc);
+            // one right-hand side (MMA false): FMA tile (an MMA would idle 7 of its 8 columns)
+            MmaAcc<A> acc;
+            acc.zero();
+            A accf[TG_O];
+            tile_zero(accf);
             for (int p = p0; p < p1; ++p) {
                 const int snc = ncoef_of(t, t.level[r.i2o_src[p]]);
                 const T *B = B0 + r.pair_cpl[p];
                 const T *X = am + r.pair_src[p] * nrhs;
                 const int64_t ps = r.pair_perm ? r.pair_perm[p] : -1;
-                if (ps < 0) {
-                    // forward: block (r, t) is nc x snc; transposed: block (t, r) is snc x nc
-                    tile_gemm(B, mode == H2B_FORWARD ? nc : snc, mode != H2B_FORWARD, adj, m0, mt, snc, nqc,
-                              [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + k]); }, Ms, Xs, acc);
+                auto prod = [&](bool kfast, auto mload, auto xload) {
+                    if constexpr (!MMA) tile_gemm_l(kfast, m0, mt, snc, nqc, mload, xload, Ms, Xs, accf);
+                    else tile_gemm_mma_l(kfast, m0, mt, snc, nqc, mload, xload, Ms, Xs, acc);
+                };
+                auto xl = [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + k]); };
+                if (ps < 0 && mode == H2B_FORWARD) {
+                    // forward: block (r, t) is nc x snc
+                    prod(false, [&](int i, int k) -> A { return wide(cj(B[i + (int64_t)k * nc], adj)); }, xl);
+                } else if (ps < 0) {
+                    // transposed: block (t, r) is snc x nc
+                    prod(true, [&](int i, int k) -> A { return wide(cj(B[k + (int64_t)i * snc], adj)); }, xl);
                 } else if (mode == H2B_FORWARD) {
                     // t[rp[i], cp[j]] = M[i, j]: out[i] += sum_j M[rp^-1[i], j] x[cp[j]]
                     // (gather / canonical product / scatter of symmetryreduceddense.jl:84-95,
                     // with the scatter folded into the row index)
                     const int *ri = m.perm + ps + nc, *cp = m.perm + ps + 2 * nc;
-                    tile_gemm_l(false, m0, mt, snc, nqc,
-                                [&](int i, int k) -> A { return wide(cj(B[ri[i] + (int64_t)k * nc], adj)); },
-                                [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + cp[k]]); },
-                                Ms, Xs, acc);
+                    prod(false, [&](int i, int k) -> A { return wide(cj(B[ri[i] + (int64_t)k * nc], adj)); },
+                         [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + cp[k]]); });
                 } else {
                     // transposed / adjoint: out[j] += sum_i op(M)[cp^-1[j], i] x[rp[i]]
                     const int *rp = m.perm + ps, *ci = m.perm + ps + 3 * snc;
-                    tile_gemm_l(true, m0, mt, snc, nqc,
-                                [&](int i, int k) -> A { return wide(cj(B[k + (int64_t)ci[i] * snc], adj)); },
-                                [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + rp[k]]); },
-                                Ms, Xs, acc);
+                    prod(true, [&](int i, int k) -> A { return wide(cj(B[k + (int64_t)ci[i] * snc], adj)); },
+                         [&](int k, int q) -> A { return wide(X[(int64_t)(q0 + q) * snc + rp[k]]); });
                 }
             }
+            if constexpr (!MMA) {
 #pragma unroll
-            for (int j = 0; j < TG_O; ++j) {
-                const int o = threadIdx.x + j * blockDim.x;
-                if (o < mt * nqc) narrow(acc[j], out[(int64_t)(q0 + o / mt) * nc + m0 + o % mt]);
+                for (int j = 0; j < TG_O; ++j) {
+                    const int o = threadIdx.x + j * blockDim.x;
+                    if (o < mt * nqc) narrow(accf[j], out[(int64_t)(q0 + o / mt) * nc + m0 + o % mt]);
+                }
+            } else {
+                mma_store(acc, mt, nqc, [&](int i, int q, A v) { narrow(v, out[(int64_t)(q0 + q) * nc + m0 + i]); });
             }
         }
     }
@@ -835,7 +966,7 @@ i2o_slot_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
 // ---------------------------------------------------------------------------------------------
 // C1: l_c = [l_c +] op(T_{level(c), sector(c)}) l_parent, op = transpose (adjoint for adjoint maps)
 // ---------------------------------------------------------------------------------------------
-template <class T>
+template <class T, bool MMA>
 __global__ void transfer_down_kernel(DMap m, DSide s, const int *__restrict__ nodes,
                                      const uint8_t *__restrict__ received, bool conjt, int nrhs,
                                      T *__restrict__ dm) {
@@ -858,17 +989,29 @@ __global__ void transfer_down_kernel(DMap m, DSide s, const int *__restrict__ no
             const int nqc = min(TG_Q, nq - q0);
             for (int m0 = 0; m0 < nout; m0 += TG_M) {
                 const int mt = min(TG_M, nout - m0);
-                A acc[TG_O];
-                tile_zero(acc);
-                tile_gemm(Tk, nin, true, conjt, m0, mt, nin, nqc,
-                          [&](int kk, int q) -> A { return wide(mp[(int64_t)(q0 + q) * nin + kk]); }, Ms, Xs, acc);
+                if constexpr (!MMA) {  // one right-hand side: FMA tile (an MMA would idle 7 of 8 columns)
+                    A acc[TG_O];
+                    tile_zero(acc);
+                    tile_gemm(Tk, nin, true, conjt, m0, mt, nin, nqc,
+                              [&](int kk, int q) -> A { return wide(mp[(int64_t)(q0 + q) * nin + kk]); }, Ms, Xs, acc);
 #pragma unroll
-                for (int j = 0; j < TG_O; ++j) {
-                    const int o = threadIdx.x + j * blockDim.x;
-                    if (o < mt * nqc) {
-                        T *dst = &mc[(int64_t)(q0 + o / mt) * nout + m0 + o % mt];
-                        narrow(acc0 ? wide(*dst) + acc[j] : acc[j], *dst);
+                    for (int j = 0; j < TG_O; ++j) {
+                        const int o = threadIdx.x + j * blockDim.x;
+                        if (o < mt * nqc) {
+                            T *dst = &mc[(int64_t)(q0 + o / mt) * nout + m0 + o % mt];
+                            narrow(acc0 ? wide(*dst) + acc[j] : acc[j], *dst);
+                        }
                     }
+                } else {
+                MmaAcc<A> acc;  // FP64 tensor cores (256 threads: 8 warps x 8 rows)
+                acc.zero();
+                tile_gemm_mma_l(true, m0, mt, nin, nqc,
+                                [&](int i, int kk) -> A { return wide(cj(Tk[kk + (int64_t)i * nin], conjt)); },
+                                [&](int kk, int q) -> A { return wide(mp[(int64_t)(q0 + q) * nin + kk]); }, Ms, Xs, acc);
+                mma_store(acc, mt, nqc, [&](int i, int q, A v) {
+                    T *dst = &mc[(int64_t)(q0 + q) * nout + m0 + i];
+                    narrow(acc0 ? wide(*dst) + v : v, *dst);
+                });
                 }
             }
         }
@@ -887,7 +1030,7 @@ __global__ void transfer_down_kernel(DMap m, DSide s, const int *__restrict__ no
 // ---------------------------------------------------------------------------------------------
 // C2: y[values] = alpha * sum_c op(C_c)^T l_c + beta * y[values]  (beta == 0 overwrites)
 // ---------------------------------------------------------------------------------------------
-template <class T, class V>
+template <class T, class V, bool MMA>
 __global__ void __launch_bounds__(256)
 leaf_disaggregate_kernel(DMap m, DSide s, const int *__restrict__ leaves, bool conjc, int nrhs,
                          const T *__restrict__ dm, V alpha, V beta, bool beta_zero, V *__restrict__ y,
@@ -904,20 +1047,37 @@ leaf_disaggregate_kernel(DMap m, DSide s, const int *__restrict__ leaves, bool c
         const int nq = min(TG_Q, nrhs - q0);
         for (int m0 = 0; m0 < nv; m0 += TG_M) {
             const int mt = min(TG_M, nv - m0);
-            A acc[TG_O];
-            tile_zero(acc);
-            for (int c = 0; c < m.ncomp; ++c)
-                tile_gemm(C + (int64_t)c * nc * nv, nc, true, conjc, m0, mt, nc, nq,
-                          [&](int k, int q) -> A { return wide(mom[((int64_t)c * nrhs + q0 + q) * nc + k]); },
-                          Ms, Xs, acc);
+            if constexpr (!MMA) {  // one right-hand side: FMA tile
+                A acc[TG_O];
+                tile_zero(acc);
+                for (int c = 0; c < m.ncomp; ++c)
+                    tile_gemm(C + (int64_t)c * nc * nv, nc, true, conjc, m0, mt, nc, nq,
+                              [&](int k, int q) -> A { return wide(mom[((int64_t)c * nrhs + q0 + q) * nc + k]); },
+                              Ms, Xs, acc);
 #pragma unroll
-            for (int j = 0; j < TG_O; ++j) {
-                const int o = threadIdx.x + j * blockDim.x;
-                if (o < mt * nq) {
-                    V *dst = &y[(int64_t)(q0 + o / mt) * ldy + s.value[v0 + m0 + o % mt]];
-                    const V v = alpha * acc[j];
-                    *dst = beta_zero ? v : v + beta * *dst;
+                for (int j = 0; j < TG_O; ++j) {
+                    const int o = threadIdx.x + j * blockDim.x;
+                    if (o < mt * nq) {
+                        V *dst = &y[(int64_t)(q0 + o / mt) * ldy + s.value[v0 + m0 + o % mt]];
+                        const V v = alpha * acc[j];
+                        *dst = beta_zero ? v : v + beta * *dst;
+                    }
                 }
+            } else {
+            MmaAcc<A> acc;  // FP64 tensor cores (256 threads: 8 warps x 8 rows)
+            acc.zero();
+            for (int c = 0; c < m.ncomp; ++c) {
+                const T *Cc = C + (int64_t)c * nc * nv;
+                tile_gemm_mma_l(true, m0, mt, nc, nq,
+                                [&](int i, int k) -> A { return wide(cj(Cc[k + (int64_t)i * nc], conjc)); },
+                                [&](int k, int q) -> A { return wide(mom[((int64_t)c * nrhs + q0 + q) * nc + k]); },
+                                Ms, Xs, acc);
+            }
+            mma_store(acc, mt, nq, [&](int i, int q, A v) {
+                V *dst = &y[(int64_t)(q0 + q) * ldy + s.value[v0 + m0 + i]];
+                const V w = alpha * v;
+                *dst = beta_zero ? w : w + beta * *dst;
+            });
             }
         }
     }
@@ -971,16 +1131,25 @@ cudaError_t launch_leaf_aggregate(bool cplx, int precision, const DMap &m, const
                                   const FarArgs &fa, const void *x, int64_t ldx, cudaStream_t st) {
     (void)maxcoef;
     if (nleaves == 0) return cudaSuccess;
+    cudaError_t err = cudaSuccess;
     if (!cplx) {
-        H2B_DISPATCH_REAL(precision,
-            leaf_aggregate_kernel<T, double><<<nleaves, 256, tile_smem<double>(), st>>>(
-                m, s, leaves, conjc, fa.nrhs, static_cast<const double *>(x), ldx, static_cast<T *>(fa.am)));
+        H2B_DISPATCH_REAL(precision, {
+            auto kern = fa.nrhs > 1 ? &leaf_aggregate_kernel<T, double, true> : &leaf_aggregate_kernel<T, double, false>;
+            err = allow_smem(kern, tile_smem<double>());
+            if (err == cudaSuccess)
+                kern<<<nleaves, 256, tile_smem<double>(), st>>>(
+                    m, s, leaves, conjc, fa.nrhs, static_cast<const double *>(x), ldx, static_cast<T *>(fa.am));
+        });
     } else {
-        H2B_DISPATCH_CPLX(precision,
-            leaf_aggregate_kernel<T, cdouble><<<nleaves, 256, tile_smem<cdouble>(), st>>>(
-                m, s, leaves, conjc, fa.nrhs, static_cast<const cdouble *>(x), ldx, static_cast<T *>(fa.am)));
+        H2B_DISPATCH_CPLX(precision, {
+            auto kern = fa.nrhs > 1 ? &leaf_aggregate_kernel<T, cdouble, true> : &leaf_aggregate_kernel<T, cdouble, false>;
+            err = allow_smem(kern, tile_smem<cdouble>());
+            if (err == cudaSuccess)
+                kern<<<nleaves, 256, tile_smem<cdouble>(), st>>>(
+                    m, s, leaves, conjc, fa.nrhs, static_cast<const cdouble *>(x), ldx, static_cast<T *>(fa.am));
+        });
     }
-    return cudaGetLastError();
+    return err != cudaSuccess ? err : cudaGetLastError();
 }
 
 cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DSide &s,
@@ -993,9 +1162,10 @@ cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DS
         using A = typename ScalarTraits<T>::Acc;
         const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? tile_smem<A>()
                                                                  : 3 * (size_t)maxsep * sizeof(A);
-        err = allow_smem(transfer_up_kernel<T>, sm);
+        auto kern = m.ncomp * fa.nrhs > 1 ? &transfer_up_kernel<T, true> : &transfer_up_kernel<T, false>;
+        err = allow_smem(kern, sm);
         if (err == cudaSuccess)
-            transfer_up_kernel<T><<<nnodes, bs, sm, st>>>(m, s, nodes, conjt, fa.nrhs, static_cast<T *>(fa.am));
+            kern<<<nnodes, bs, sm, st>>>(m, s, nodes, conjt, fa.nrhs, static_cast<T *>(fa.am));
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
@@ -1107,14 +1277,18 @@ cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &rec
     const bool diag = m.coupling_kind == H2B_COUPLING_DIAGONAL;
     const int bs = toep ? block_for(m.half_spectrum ? maxhalf : maxtsize, 32, 512)
                         : (diag ? block_for(maxcoef, 64, 256) : 256);
+    cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using S = typename ScalarTraits<T>::Complex;
         const size_t sm = (toep || diag) ? 0 : tile_smem<typename ScalarTraits<T>::Acc>();
-        i2o_kernel<T><<<nnodes, bs, sm, st>>>(m, recv, src, nodes, fa.mode, fa.nrhs,
-                                              static_cast<const T *>(fa.am), static_cast<T *>(fa.dm),
-                                              static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
+        auto kern = m.ncomp * fa.nrhs > 1 ? &i2o_kernel<T, true> : &i2o_kernel<T, false>;
+        err = allow_smem(kern, sm);
+        if (err == cudaSuccess)
+            kern<<<nnodes, bs, sm, st>>>(m, recv, src, nodes, fa.mode, fa.nrhs,
+                                                  static_cast<const T *>(fa.am), static_cast<T *>(fa.dm),
+                                                  static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
     });
-    return cudaGetLastError();
+    return err != cudaSuccess ? err : cudaGetLastError();
 }
 
 cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const DSide &recv,
@@ -1152,9 +1326,10 @@ cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const 
         using A = typename ScalarTraits<T>::Acc;
         const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? tile_smem<A>()
                                                                  : 2 * (size_t)maxsep * sizeof(A);
-        err = allow_smem(transfer_down_kernel<T>, sm);
+        auto kern = m.ncomp * fa.nrhs > 1 ? &transfer_down_kernel<T, true> : &transfer_down_kernel<T, false>;
+        err = allow_smem(kern, sm);
         if (err == cudaSuccess)
-            transfer_down_kernel<T><<<nnodes, bs, sm, st>>>(m, s, nodes, received, conjt, fa.nrhs,
+            kern<<<nnodes, bs, sm, st>>>(m, s, nodes, received, conjt, fa.nrhs,
                                                            static_cast<T *>(fa.dm));
     });
     return err != cudaSuccess ? err : cudaGetLastError();
@@ -1166,20 +1341,29 @@ cudaError_t launch_leaf_disaggregate(bool cplx, int precision, const DMap &m, co
                                      cudaStream_t st) {
     if (nleaves == 0) return cudaSuccess;
     const int bs = 256;
+    cudaError_t err = cudaSuccess;
     if (!cplx) {
         const bool bz = beta.x == 0.0;
-        H2B_DISPATCH_REAL(precision,
-            leaf_disaggregate_kernel<T, double><<<nleaves, bs, tile_smem<double>(), st>>>(
-                m, s, leaves, conjc, fa.nrhs, static_cast<const T *>(fa.dm), alpha.x, beta.x, bz,
-                static_cast<double *>(y), ldy));
+        H2B_DISPATCH_REAL(precision, {
+            auto kern = fa.nrhs > 1 ? &leaf_disaggregate_kernel<T, double, true> : &leaf_disaggregate_kernel<T, double, false>;
+            err = allow_smem(kern, tile_smem<double>());
+            if (err == cudaSuccess)
+                kern<<<nleaves, bs, tile_smem<double>(), st>>>(
+                    m, s, leaves, conjc, fa.nrhs, static_cast<const T *>(fa.dm), alpha.x, beta.x, bz,
+                    static_cast<double *>(y), ldy);
+        });
     } else {
         const bool bz = beta.x == 0.0 && beta.y == 0.0;
-        H2B_DISPATCH_CPLX(precision,
-            leaf_disaggregate_kernel<T, cdouble><<<nleaves, bs, tile_smem<cdouble>(), st>>>(
-                m, s, leaves, conjc, fa.nrhs, static_cast<const T *>(fa.dm), alpha, beta, bz,
-                static_cast<cdouble *>(y), ldy));
+        H2B_DISPATCH_CPLX(precision, {
+            auto kern = fa.nrhs > 1 ? &leaf_disaggregate_kernel<T, cdouble, true> : &leaf_disaggregate_kernel<T, cdouble, false>;
+            err = allow_smem(kern, tile_smem<cdouble>());
+            if (err == cudaSuccess)
+                kern<<<nleaves, bs, tile_smem<cdouble>(), st>>>(
+                    m, s, leaves, conjc, fa.nrhs, static_cast<const T *>(fa.dm), alpha, beta, bz,
+                    static_cast<cdouble *>(y), ldy);
+        });
     }
-    return cudaGetLastError();
+    return err != cudaSuccess ? err : cudaGetLastError();
 }
 
 cudaError_t launch_zero_columns(bool cplx, int nrhs, int64_t n, void *y, int64_t ldy, cudaStream_t st) {

@@ -288,6 +288,142 @@ near_rows_mma_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const dou
     }
 }
 
+// Gather for the tensor-core kernel below: the right-hand sides of input dof value[pos] as one
+// contiguous row, xp[pos * R + q] = x[(r0 + q) * ldx + value[pos]] (zero for q >= rc), so a warp
+// reads its 32-column x chunk as one 4 KB range instead of 512 scattered elements.
+template <int R>
+__global__ void near_gather_kernel(const int *__restrict__ value, int nvals, int r0, int rc,
+                                   const double *__restrict__ x, int64_t ldx, double *__restrict__ xp) {
+    const int64_t total = (int64_t)nvals * R;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int pos = (int)(e / R), q = (int)(e % R);
+        xp[e] = q < rc ? x[(int64_t)(r0 + q) * ldx + value[pos]] : 0.0;
+    }
+}
+
+// Real near blocks, 8 or 16 right-hand sides, FP64 tensor cores, second form. Warps 0-3 take the
+// first 32 rows of a 64-row pass and warps 4-7 the next 32; each warp owns 4 row tiles and reads
+// them as 16-byte pairs: fragment row g of tile t is the block row 4g + t of its half, so lane
+// (g, k) loads rows 4g..4g+3 of column k with two 16-byte loads, the next column step's loads in
+// flight while the current step's 4 x NT MMAs issue. The x chunk of a unit comes from the
+// gathered rows of near_gather_kernel. Partial rows meet in shared memory (reusing the x chunks)
+// and are summed over the 4 warps of each half.
+template <int NT>
+__global__ void __launch_bounds__(NEAR_WARPS * 32, 3)
+near_rows_mma2_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const double *__restrict__ xp,
+                      double *__restrict__ y, int64_t ldy, double alpha, double beta, bool beta_zero) {
+    constexpr int R = 8 * NT;
+    constexpr int XS = R + 4;  // x chunk row stride (doubles)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int g = blockIdx.x;
+    const int leaf = op.grp_leaf[g];
+    const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
+    const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g4 = lane >> 2, t4 = lane & 3;
+    const int half = warp >> 2, wq = warp & 3;
+    double *xs = reinterpret_cast<double *>(smem_raw) + warp * 32 * XS;
+    double *part = reinterpret_cast<double *>(smem_raw);  // [8 warps][32 rows][R], after the units
+    const double *D = static_cast<const double *>(op.data);
+    const int ld = nr + (nr & 1);
+    for (int p0 = 0; p0 < nr; p0 += 64) {
+        const int rows0 = p0 + 32 * half;          // this warp's first row
+        const bool active = rows0 < nr;            // warp-uniform
+        const int lr = rows0 + 4 * g4;             // this lane's first row
+        const bool ok01 = lr < nr, ok23 = lr + 2 < nr;
+        double acc[4][NT][2];
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+            for (int u = 0; u < NT; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
+        int unit = 0;
+        for (int bb = b0; bb < b1 && active; ++bb) {
+            const int blk = op.grp_blk[bb];
+            const int inl = op.blk_in[blk];
+            const int c0 = ins.value_ptr[inl], nc = ins.value_ptr[inl + 1] - c0;
+            const double *Bl = D + op.blk_off[blk] + lr;
+            for (int j0 = 0; j0 < nc; j0 += 32, ++unit) {
+                if (unit % 4 != wq) continue;
+                __syncwarp();
+                for (int e = lane; e < 32 * R / 2; e += 32) {  // 16-byte pieces of the chunk
+                    const int col = (2 * e) / R, q = (2 * e) % R;
+                    double2 v = make_double2(0.0, 0.0);
+                    if (j0 + col < nc) v = __ldg(reinterpret_cast<const double2 *>(xp + (int64_t)(c0 + j0 + col) * R + q));
+                    xs[col * XS + q] = v.x;
+                    xs[col * XS + q + 1] = v.y;
+                }
+                __syncwarp();
+                const int jn = min(32, nc - j0);
+                auto load = [&](int kk, double (&a)[4]) {
+                    const int col = kk + t4;
+                    const double *pc = Bl + (int64_t)(j0 + col) * ld;
+                    double2 v01 = make_double2(0.0, 0.0), v23 = make_double2(0.0, 0.0);
+                    if (col < jn && ok01) v01 = __ldcs(reinterpret_cast<const double2 *>(pc));
+                    if (col < jn && ok23) v23 = __ldcs(reinterpret_cast<const double2 *>(pc + 2));
+                    a[0] = v01.x;
+                    a[1] = v01.y;
+                    a[2] = v23.x;
+                    a[3] = v23.y;
+                };
+                double a[4], an[4];
+                load(0, a);
+                for (int kk = 0; kk < jn; kk += 4) {
+                    if (kk + 4 < jn) load(kk + 4, an);
+                    double b[NT];
+#pragma unroll
+                    for (int u = 0; u < NT; ++u) b[u] = xs[(kk + t4) * XS + 8 * u + g4];
+#pragma unroll
+                    for (int t = 0; t < 4; ++t)
+#pragma unroll
+                        for (int u = 0; u < NT; ++u) dmma(acc[t][u], a[t], b[u]);
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) a[t] = an[t];
+                }
+            }
+        }
+        __syncthreads();  // every warp is done with its x chunks: reuse them for the partial rows
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+            for (int u = 0; u < NT; ++u)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    part[(warp * 32 + 4 * g4 + t) * R + 8 * u + 2 * t4 + h] = acc[t][u][h];
+        __syncthreads();
+        const int rows = min(64, nr - p0);
+        for (int e = threadIdx.x; e < rows * rc; e += blockDim.x) {
+            const int i = e / rc, q = e % rc;
+            const int hf = i >> 5, li = i & 31;
+            double sum = 0.0;
+#pragma unroll
+            for (int w = 0; w < 4; ++w) sum += part[((hf * 4 + w) * 32 + li) * R + q];
+            double *o = &y[(int64_t)(r0 + q) * ldy + outs.value[o0 + p0 + i]];
+            const double v = alpha * sum;
+            *o = beta_zero ? v : v + beta * *o;
+        }
+        __syncthreads();
+    }
+}
+
+template <int NT>
+cudaError_t launch_rows_mma2(const NearOp &op, const DSide &outs, const DSide &ins, int r0, int rc,
+                             const double *x, int64_t ldx, double *xp, double *y, int64_t ldy, double alpha,
+                             double beta, bool bz, cudaStream_t st) {
+    constexpr int R = 8 * NT;
+    const int nvals = ins.nvalues;
+    near_gather_kernel<R><<<std::max(1, std::min(148 * 8, (int)(((int64_t)nvals * R + 255) / 256))), 256, 0, st>>>(
+        ins.value, nvals, r0, rc, x, ldx, xp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t sm = (size_t)NEAR_WARPS * 32 * (R + 4) * sizeof(double);  // >= the partial rows
+    static_assert(32 * (8 + 4) >= 32 * 8 && 32 * (16 + 4) >= 32 * 16, "partial rows fit the x chunks");
+    if (sm > 48 * 1024) e = cudaFuncSetAttribute(near_rows_mma2_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    near_rows_mma2_kernel<NT><<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, r0, rc, xp, y, ldy, alpha,
+                                                                       beta, bz);
+    return cudaGetLastError();
+}
+
 template <int NT>
 cudaError_t launch_rows_mma(const NearOp &op, const DSide &outs, const DSide &ins, int r0, int rc,
                             const double *x, int64_t ldx, double *y, int64_t ldy, double alpha, double beta,
@@ -541,20 +677,23 @@ cudaError_t launch_rows_t(const NearOp &op, const DSide &outs, const DSide &ins,
 template <class V>
 cudaError_t near_apply_t(const NearOp &op, const DSide &outs, const DSide &ins, bool cjg, int nrhs,
                          const V *x, int64_t ldx, V *y, int64_t ldy, V alpha, V beta, bool bz,
-                         cudaStream_t st) {
+                         double *xp, cudaStream_t st) {
     if (op.ngroups == 0) return cudaSuccess;
     for (int r0 = 0; r0 < nrhs; r0 += 16) {
         const int rc = std::min(16, nrhs - r0);
         cudaError_t e;
         if constexpr (std::is_same<V, double>::value) {
             // real blocks, 8 or more right-hand sides: FP64 tensor-core MMA
+            // with a gather buffer (workspaces of 8 or more right-hand sides): the second form
             if (rc > 8) {
-                e = launch_rows_mma<2>(op, outs, ins, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+                e = xp ? launch_rows_mma2<2>(op, outs, ins, r0, rc, x, ldx, xp, y, ldy, alpha, beta, bz, st)
+                       : launch_rows_mma<2>(op, outs, ins, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
                 if (e != cudaSuccess) return e;
                 continue;
             }
             if (rc == 8) {
-                e = launch_rows_mma<1>(op, outs, ins, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+                e = xp ? launch_rows_mma2<1>(op, outs, ins, r0, rc, x, ldx, xp, y, ldy, alpha, beta, bz, st)
+                       : launch_rows_mma<1>(op, outs, ins, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
                 if (e != cudaSuccess) return e;
                 continue;
             }
@@ -603,7 +742,7 @@ cudaError_t launch_near_symcheck(bool cplx, const void *src, const int64_t *off,
 
 cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &test, const DSide &trial,
                         int nrhs, const void *x, int64_t ldx, void *y, int64_t ldy, cdouble alpha,
-                        cdouble beta, cudaStream_t st) {
+                        cdouble beta, void *xp, cudaStream_t st) {
     const bool fwd_op = mode == H2B_FORWARD || n.symmetric;
     const NearOp &op = fwd_op ? n.fwd : n.tr;
     const DSide &outs = fwd_op ? test : trial;
@@ -629,9 +768,10 @@ cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &test, 
     if (cplx)
         return near_apply_t<cdouble>(op, outs, ins, cjg, nrhs, static_cast<const cdouble *>(x), ldx,
                                      static_cast<cdouble *>(y), ldy, alpha, beta,
-                                     beta.x == 0.0 && beta.y == 0.0, st);
+                                     beta.x == 0.0 && beta.y == 0.0, nullptr, st);
     return near_apply_t<double>(op, outs, ins, false, nrhs, static_cast<const double *>(x), ldx,
-                                static_cast<double *>(y), ldy, alpha.x, beta.x, beta.x == 0.0, st);
+                                static_cast<double *>(y), ldy, alpha.x, beta.x, beta.x == 0.0,
+                                static_cast<double *>(xp), st);
 }
 
 }  // namespace h2b
