@@ -194,98 +194,12 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
     }
 }
 
-// Real near blocks with 8 or 16 right-hand sides on the FP64 tensor cores (mma.sync m8n8k4 f64).
-// A warp owns 64 rows (eight 8-row tiles) and all R = 8 * NT right-hand sides; per step of four
-// columns it loads its A fragments (the near block, one value per lane per row tile) straight
-// from HBM, its B fragments (x) from the warp's shared-memory chunk, and issues 8 * NT MMAs.
-// Fragment layout (PTX ISA, m8n8k4 .f64): A[lane/4][lane%4], B[lane%4][lane/4],
-// C[lane/4][2*(lane%4) + i]. Same block walk and reduction as near_rows_kernel.
+// FP64 tensor-core MMA, m8n8k4 (PTX ISA fragment layout for .f64: A[lane/4][lane%4],
+// B[lane%4][lane/4], C[lane/4][2*(lane%4) + i]).
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(c[0]), "+d"(c[1])
                  : "d"(a), "d"(b));
-}
-
-template <int NT>
-__global__ void __launch_bounds__(NEAR_WARPS * 32, 2)
-near_rows_mma_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const double *__restrict__ x,
-                     int64_t ldx, double *__restrict__ y, int64_t ldy, double alpha, double beta,
-                     bool beta_zero) {
-    constexpr int R = 8 * NT;
-    constexpr int XS = R + 4;  // padded row of the x chunk
-    constexpr int RPP = 64;
-    extern __shared__ unsigned char smem_raw[];
-    const int g = blockIdx.x;
-    const int leaf = op.grp_leaf[g];
-    const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
-    const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int g4 = lane >> 2, t4 = lane & 3;
-    double *xs = reinterpret_cast<double *>(smem_raw) + warp * 32 * XS;
-    double *part = reinterpret_cast<double *>(smem_raw) + NEAR_WARPS * 32 * XS;  // [NEAR_WARPS][RPP][R]
-    const double *D = static_cast<const double *>(op.data);
-    const int ld = nr + (nr & 1);
-    for (int p0 = 0; p0 < nr; p0 += RPP) {
-        double acc[8][NT][2];
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-#pragma unroll
-            for (int u = 0; u < NT; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
-        int unit = 0;
-        for (int bb = b0; bb < b1; ++bb) {
-            const int blk = op.grp_blk[bb];
-            const int inl = op.blk_in[blk];
-            const int c0 = ins.value_ptr[inl], nc = ins.value_ptr[inl + 1] - c0;
-            const double *B = D + op.blk_off[blk];
-            for (int j0 = 0; j0 < nc; j0 += 32, ++unit) {
-                if (unit % NEAR_WARPS != warp) continue;
-                __syncwarp();
-                {
-                    const int jl = j0 + lane;
-                    const int dof = jl < nc ? ins.value[c0 + jl] : 0;
-#pragma unroll
-                    for (int q = 0; q < R; ++q)
-                        xs[lane * XS + q] = (jl < nc && q < rc) ? x[(int64_t)(r0 + q) * ldx + dof] : 0.0;
-                }
-                __syncwarp();
-                const int jn = min(32, nc - j0);
-                for (int kk = 0; kk < jn; kk += 4) {
-                    const int col = kk + t4;
-                    const bool cv = col < jn;
-                    const double *bc = B + (int64_t)(j0 + col) * ld + p0 + g4;
-                    double a[8];
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) a[t] = (cv && p0 + 8 * t + g4 < nr) ? __ldcs(bc + 8 * t) : 0.0;
-                    double b[NT];
-#pragma unroll
-                    for (int u = 0; u < NT; ++u) b[u] = cv ? xs[col * XS + 8 * u + g4] : 0.0;
-#pragma unroll
-                    for (int t = 0; t < 8; ++t)
-#pragma unroll
-                        for (int u = 0; u < NT; ++u) dmma(acc[t][u], a[t], b[u]);
-                }
-            }
-        }
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-#pragma unroll
-            for (int u = 0; u < NT; ++u)
-#pragma unroll
-                for (int i = 0; i < 2; ++i)
-                    part[(warp * RPP + 8 * t + g4) * R + 8 * u + 2 * t4 + i] = acc[t][u][i];
-        __syncthreads();
-        const int rows = min(RPP, nr - p0);
-        for (int e = threadIdx.x; e < rows * rc; e += blockDim.x) {
-            const int i = e / rc, q = e % rc;
-            double sum = 0.0;
-#pragma unroll
-            for (int w = 0; w < NEAR_WARPS; ++w) sum += part[(w * RPP + i) * R + q];
-            double *o = &y[(int64_t)(r0 + q) * ldy + outs.value[o0 + p0 + i]];
-            const double v = alpha * sum;
-            *o = beta_zero ? v : v + beta * *o;
-        }
-        __syncthreads();
-    }
 }
 
 // Gather for the tensor-core kernel below: the right-hand sides of input dof value[pos] as one
@@ -301,7 +215,7 @@ __global__ void near_gather_kernel(const int *__restrict__ value, int nvals, int
     }
 }
 
-// Real near blocks, 8 or 16 right-hand sides, FP64 tensor cores, second form. Warps 0-3 take the
+// Real near blocks, 8 or 16 right-hand sides, on the FP64 tensor cores. Warps 0-3 take the
 // first 32 rows of a 64-row pass and warps 4-7 the next 32; each warp owns 4 row tiles and reads
 // them as 16-byte pairs: fragment row g of tile t is the block row 4g + t of its half, so lane
 // (g, k) loads rows 4g..4g+3 of column k with two 16-byte loads, the next column step's loads in
@@ -310,7 +224,7 @@ __global__ void near_gather_kernel(const int *__restrict__ value, int nvals, int
 // and are summed over the 4 warps of each half.
 template <int NT>
 __global__ void __launch_bounds__(NEAR_WARPS * 32, 3)
-near_rows_mma2_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const double *__restrict__ xp,
+near_rows_mma_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const double *__restrict__ xp,
                       double *__restrict__ y, int64_t ldy, double alpha, double beta, bool beta_zero) {
     constexpr int R = 8 * NT;
     constexpr int XS = R + 4;  // x chunk row stride (doubles)
@@ -406,7 +320,7 @@ near_rows_mma2_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const do
 }
 
 template <int NT>
-cudaError_t launch_rows_mma2(const NearOp &op, const DSide &outs, const DSide &ins, int r0, int rc,
+cudaError_t launch_rows_mma(const NearOp &op, const DSide &outs, const DSide &ins, int r0, int rc,
                              const double *x, int64_t ldx, double *xp, double *y, int64_t ldy, double alpha,
                              double beta, bool bz, cudaStream_t st) {
     constexpr int R = 8 * NT;
@@ -417,27 +331,13 @@ cudaError_t launch_rows_mma2(const NearOp &op, const DSide &outs, const DSide &i
     if (e != cudaSuccess) return e;
     const size_t sm = (size_t)NEAR_WARPS * 32 * (R + 4) * sizeof(double);  // >= the partial rows
     static_assert(32 * (8 + 4) >= 32 * 8 && 32 * (16 + 4) >= 32 * 16, "partial rows fit the x chunks");
-    if (sm > 48 * 1024) e = cudaFuncSetAttribute(near_rows_mma2_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (sm > 48 * 1024) e = cudaFuncSetAttribute(near_rows_mma_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    near_rows_mma2_kernel<NT><<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, r0, rc, xp, y, ldy, alpha,
+    near_rows_mma_kernel<NT><<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, r0, rc, xp, y, ldy, alpha,
                                                                        beta, bz);
     return cudaGetLastError();
 }
 
-template <int NT>
-cudaError_t launch_rows_mma(const NearOp &op, const DSide &outs, const DSide &ins, int r0, int rc,
-                            const double *x, int64_t ldx, double *y, int64_t ldy, double alpha, double beta,
-                            bool bz, cudaStream_t st) {
-    constexpr int R = 8 * NT;
-    const size_t sm = (size_t)NEAR_WARPS * (32 * (R + 4) + 64 * R) * sizeof(double);
-    cudaError_t e = cudaSuccess;
-    if (sm > 48 * 1024)
-        e = cudaFuncSetAttribute(near_rows_mma_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    near_rows_mma_kernel<NT><<<op.ngroups, NEAR_WARPS * 32, sm, st>>>(op, outs, ins, r0, rc, x, ldx, y, ldy,
-                                                                       alpha, beta, bz);
-    return cudaGetLastError();
-}
 
 // Matrix-free near field ---------------------------------------------------------------------
 // The point kernels of H2B_NEAR_LAPLACE / H2B_NEAR_HELMHOLTZ: the entry of (output dof i, input
@@ -684,16 +584,14 @@ cudaError_t near_apply_t(const NearOp &op, const DSide &outs, const DSide &ins, 
         cudaError_t e;
         if constexpr (std::is_same<V, double>::value) {
             // real blocks, 8 or more right-hand sides: FP64 tensor-core MMA
-            // with a gather buffer (workspaces of 8 or more right-hand sides): the second form
-            if (rc > 8) {
-                e = xp ? launch_rows_mma2<2>(op, outs, ins, r0, rc, x, ldx, xp, y, ldy, alpha, beta, bz, st)
-                       : launch_rows_mma<2>(op, outs, ins, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+            // 8 or more right-hand sides (workspaces that size carry the gather buffer): tensor cores
+            if (rc > 8 && xp) {
+                e = launch_rows_mma<2>(op, outs, ins, r0, rc, x, ldx, xp, y, ldy, alpha, beta, bz, st);
                 if (e != cudaSuccess) return e;
                 continue;
             }
-            if (rc == 8) {
-                e = xp ? launch_rows_mma2<1>(op, outs, ins, r0, rc, x, ldx, xp, y, ldy, alpha, beta, bz, st)
-                       : launch_rows_mma<1>(op, outs, ins, r0, rc, x, ldx, y, ldy, alpha, beta, bz, st);
+            if (rc == 8 && xp) {
+                e = launch_rows_mma<1>(op, outs, ins, r0, rc, x, ldx, xp, y, ldy, alpha, beta, bz, st);
                 if (e != cudaSuccess) return e;
                 continue;
             }
