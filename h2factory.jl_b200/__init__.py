@@ -15,5 +15,6 @@ from . import trees, _abi  # noqa: F401
 from .core import (H2Core, DeviceCore, H2Workspace, OrientedMap, adjoint, farmul_, flatten,  # noqa: F401
                    map_blob, mul_, nearmul_, read_blob, save_map, similarworkspace, transpose)
 from . import methods  # noqa: F401
+from . import batch  # noqa: F401
 from ._abi import (H2B_ADJOINT as ADJOINT, H2B_FORWARD as FORWARD,  # noqa: F401
                    H2B_TRANSPOSE as TRANSPOSE, H2BError, WorkspaceBusyError)

@@ -997,6 +997,7 @@ h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **
         CUDA_TRY(cudaGetDeviceCount(&ndev));
         if (device < 0 || device >= ndev) return fail(H2B_ERR_INVALID, "device %d not present", device);
         DeviceGuard guard(device);
+        (void)cudaGetLastError();  // a non-sticky error left by other code is not this call's
         h2b_core *c = new h2b_core();
         c->device = device;
         c->field = desc->field;
@@ -1023,6 +1024,7 @@ h2b_status h2b_core_destroy(h2b_core *core) {
     DeviceGuard guard(core->device);
     core->release();
     delete core;
+    (void)cudaGetLastError();  // teardown reports nothing to later calls
     return H2B_OK;
 }
 
@@ -1049,6 +1051,7 @@ h2b_status h2b_workspace_destroy(h2b_workspace *ws) {
     if (ws->ev_join) cudaEventDestroy(ws->ev_join);
     if (ws->ev_done) cudaEventDestroy(ws->ev_done);
     delete ws;
+    (void)cudaGetLastError();  // teardown reports nothing to later calls
     return H2B_OK;
 }
 
@@ -1057,6 +1060,7 @@ h2b_status h2b_workspace_create(h2b_core *core, int32_t max_nrhs, h2b_workspace 
     if (max_nrhs < 1) return fail(H2B_ERR_INVALID, "max_nrhs must be >= 1");
     *out = nullptr;
     DeviceGuard guard(core->device);
+    (void)cudaGetLastError();  // a non-sticky error left by other code is not this call's
     h2b_workspace *ws = new (std::nothrow) h2b_workspace();
     if (!ws) return fail(H2B_ERR_NOMEM, "host allocation failed");
     ws->core = core;
@@ -1183,9 +1187,14 @@ h2b_status run(h2b_workspace *ws, Kind kind, int32_t mode, int32_t nrhs, const v
     BusyGuard busy(ws->busy);
     if (take_busy && !busy.ok) return fail(H2B_BUSY, "workspace is in use by another call");
     DeviceGuard guard(c->device);
+    (void)cudaGetLastError();  // a non-sticky error left by other code is not this call's
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // serialise with the previous call on this workspace, whatever stream it used
-    CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_done, 0));
+    // serialise with the previous call on this workspace, whatever stream it used; inside a
+    // stream capture the captured order does that, and the event of an earlier, uncaptured call
+    // cannot be waited on
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+    if (cap == cudaStreamCaptureStatusNone) CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_done, 0));
     const cdouble a = alpha ? cdouble{alpha[0], alpha[1]} : cdouble{1.0, 0.0};
     const cdouble b = beta ? cdouble{beta[0], beta[1]} : cdouble{0.0, 0.0};
     const cdouble aA = c->alpha[mode];
@@ -1211,7 +1220,7 @@ h2b_status run(h2b_workspace *ws, Kind kind, int32_t mode, int32_t nrhs, const v
         s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(aA, a), cdouble{1.0, 0.0}, st, ws->ev_join);
     }
     if (s) return s;
-    CUDA_TRY(cudaEventRecord(ws->ev_done, st));
+    if (cap == cudaStreamCaptureStatusNone) CUDA_TRY(cudaEventRecord(ws->ev_done, st));
     return H2B_OK;
 }
 
