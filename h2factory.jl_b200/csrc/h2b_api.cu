@@ -514,6 +514,7 @@ h2b_status build_sibling_groups(h2b_core *c, const h2b_side_desc &s, SideHost &h
                 row[sl] = (int)ko;
             }
         }
+        if (gslen[gi] > 512) return H2B_OK;  // one thread per stored frequency: per-node kernel
         for (auto &kv : bysrc) {
             gsrc.push_back(other_spec_off[kv.first]);
             gkof.insert(gkof.end(), kv.second.begin(), kv.second.end());

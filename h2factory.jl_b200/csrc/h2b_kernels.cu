@@ -843,16 +843,18 @@ __global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, cons
 // L1). Per complex multiply-add this moves one kernel value per QB right-hand sides and one source
 // value per group instead of one of each per pair.
 // ---------------------------------------------------------------------------------------------
-template <class T, int QB>
+// SL child slots per thread (8: one thread per frequency; 4: two threads per frequency, half
+// the accumulators), U source entries per step with every load issued before the arithmetic.
+template <class T, int QB, int SL, int U>
 __global__ void __launch_bounds__(512)
-i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
+i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs, int et,
                    const typename ScalarTraits<T>::Complex *__restrict__ as,
                    typename ScalarTraits<T>::Complex *__restrict__ ds) {
     using S = typename ScalarTraits<T>::Complex;
     const int gi = blockIdx.x;
     const int q0 = blockIdx.y * QB;
     const int nq = m.ncomp * nrhs;
-    const int e = threadIdx.x;
+    const int e = threadIdx.x % et, s0 = (threadIdx.x / et) * SL;  // frequency, first slot
     const int slen = g.slen[gi];
     if (e >= slen) return;  // no barriers below
     const bool adj = mode == H2B_ADJOINT;
@@ -861,36 +863,33 @@ i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
     // accumulated in the storage type: FP64 in the FP64 form; FP32 in the FP32 form, whose sums of
     // at most one interaction list (189 pairs in a uniform tree) per frequency keep the product
     // within 3.2e-7 of the FP64 one on the benchmark map (2.2e-7 with FP64 sums)
-    S acc[8][QB];
+    S acc[SL][QB];
 #pragma unroll
-    for (int sl = 0; sl < 8; ++sl)
+    for (int sl = 0; sl < SL; ++sl)
 #pragma unroll
         for (int q = 0; q < QB; ++q) acc[sl][q] = S{};
-    // U source entries per step (two for one right-hand side, where registers allow), every load
-    // issued before the arithmetic that uses it
-    constexpr int U = QB == 1 ? 2 : 1;
     for (int k = k0; k < k1; k += U) {
         S sv[U][QB];
-        int ko[U][8];
+        int ko[U][SL];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const bool ok = k + u < k1;
-            const int *kof = g.kof + (int64_t)(ok ? k + u : k) * 8;
+            const int *kof = g.kof + (int64_t)(ok ? k + u : k) * 8 + s0;
 #pragma unroll
-            for (int sl = 0; sl < 8; ++sl) ko[u][sl] = ok ? kof[sl] : -1;
+            for (int sl = 0; sl < SL; ++sl) ko[u][sl] = ok ? kof[sl] : -1;
             const S *sp = as + g.src_off[ok ? k + u : k] * nrhs + (int64_t)q0 * slen + e;
 #pragma unroll
             for (int q = 0; q < QB; ++q) sv[u][q] = q0 + q < nq ? sp[(int64_t)q * slen] : S{};
         }
-        S kvs[U][8];
+        S kvs[U][SL];
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int sl = 0; sl < 8; ++sl) kvs[u][sl] = ko[u][sl] >= 0 ? K0[ko[u][sl] + e] : S{};
+            for (int sl = 0; sl < SL; ++sl) kvs[u][sl] = ko[u][sl] >= 0 ? K0[ko[u][sl] + e] : S{};
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int sl = 0; sl < 8; ++sl) {
+            for (int sl = 0; sl < SL; ++sl) {
                 if (ko[u][sl] >= 0) {
                     const S kv = cj(kvs[u][sl], adj);
 #pragma unroll
@@ -899,8 +898,8 @@ i2o_sibling_kernel(DMap m, DSide r, SibGroups g, int mode, int nrhs,
             }
     }
 #pragma unroll
-    for (int sl = 0; sl < 8; ++sl) {
-        const int rv = g.recv[gi * 8 + sl];
+    for (int sl = 0; sl < SL; ++sl) {
+        const int rv = g.recv[gi * 8 + s0 + sl];
         if (rv < 0) continue;
         S *out = ds + r.spec_off[rv] * nrhs + (int64_t)q0 * slen + e;
 #pragma unroll
@@ -1301,16 +1300,24 @@ cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const D
         // several right-hand sides per CTA share each kernel value load (one-wide blocks reload
         // them per right-hand side, which costs more than the lower occupancy of the wider block):
         // four with FP32 accumulators, two with FP64 ones (four would spill)
-        constexpr int QB = sizeof(typename ScalarTraits<T>::Real) == 4 ? 4 : 2;
+        constexpr bool f32 = sizeof(typename ScalarTraits<T>::Real) == 4;
+        constexpr int QB = f32 ? 4 : 2;
         // one right-hand side: the (slot, frequency) form (2 % faster on the benchmark map);
         // blocks of right-hand sides: the frequency-per-thread form, which reuses each source
         // value from registers for the 8 slots (7 % faster than the slot form at 16)
         if (nq == 1)
             i2o_slot_kernel<T, 1, 4><<<dim3(g.ngroups, (maxslen + 31) / 32, 1), 256, 0, st>>>(
                 m, recv, g, fa.mode, fa.nrhs, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
-        else
-            i2o_sibling_kernel<T, QB><<<dim3(g.ngroups, (nq + QB - 1) / QB), bs, 0, st>>>(
-                m, recv, g, fa.mode, fa.nrhs, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
+        else if (f32 && maxslen <= 256) {
+            // FP32: two threads per frequency, 4 slots x 8 right-hand sides each (3 % faster than
+            // 8 slots x 4 on the benchmark map; unrolling entries or 2-wide blocks were slower)
+            const int et = block_for(maxslen, 32, 256);
+            i2o_sibling_kernel<T, 8, 4, 1><<<dim3(g.ngroups, (nq + 7) / 8), 2 * et, 0, st>>>(
+                m, recv, g, fa.mode, fa.nrhs, et, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
+        } else {
+            i2o_sibling_kernel<T, QB, 8, 1><<<dim3(g.ngroups, (nq + QB - 1) / QB), bs, 0, st>>>(
+                m, recv, g, fa.mode, fa.nrhs, bs, static_cast<const S *>(fa.as), static_cast<S *>(fa.ds));
+        }
     });
     return cudaGetLastError();
 }
