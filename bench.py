@@ -86,13 +86,15 @@ def build_core(n=262144, depth=5, p=4, seed=0, device="cuda:0", precision="fp64"
     return h2, core
 
 
-def launches_per_step(core, mode: int) -> int:
+def launches_per_step(core, mode: int, nrhs: int = 1) -> int:
     """Kernels one h2b_matvec enqueues (same node-list logic as the library)."""
     agg = core.plans.trial if mode == 0 else core.plans.test
     dis = core.plans.test if mode == 0 else core.plans.trial
     tree = core.trial if mode == 0 else core.test
     dtree = core.test if mode == 0 else core.trial
     count = 1  # near
+    if core.field == "real" and nrhs >= 8:
+        count += 1  # gather of the x rows for the tensor-core near kernel
     count += 1  # leaf aggregation
     for st in range(agg.agg_level.size):
         nodes = agg.agg_node[agg.agg_ptr[st]:agg.agg_ptr[st + 1]]
@@ -417,7 +419,8 @@ def gpu_arm(args, rank, world, local_rank):
     achieved = near_bytes / (near_ms * 1e-3) / 1e9
     workload = WORKLOAD if (args.n, args.depth) == (262144, 5) else f"toeplitz-laplace-N{args.n}-depth{args.depth}-p4"
     traffic = traffic_table().get(("near_rows_kernel", workload))
-    launches = (sum(launches_per_step(core, i % 2) for i in range(args.steps)) * 2)
+    launches = sum(launches_per_step(core, i % 2, 1) + launches_per_step(core, i % 2, nserve)
+                   for i in range(args.steps))
     plain_rate = job_rate(args.steps, world, tot_p)
     served_rate = job_rate(args.steps * nserve, world, tot_s)
     line = {
@@ -511,6 +514,68 @@ def core_with_host_near(core, near_host):
     return c
 
 
+def sphere_core(n, device, precision="fp64"):
+    """The sphere configuration's map at `n` points: Fibonacci sphere (radius 0.45 in the unit
+    cube) with jitter 0.1 x spacing, leaves <= 128 points, Helmholtz k = 8 pi x 0.45 (the unit
+    sphere's electrical size), Chebyshev p = 6, symmetry-reduced couplings, near blocks assembled
+    on the device."""
+    h2 = _package()
+    from h2factory_b200 import assembly, methods, trees
+
+    rng = np.random.default_rng(0)
+    i = np.arange(n) + 0.5
+    phi, th = np.arccos(1 - 2 * i / n), np.pi * (1 + 5 ** 0.5) * i
+    p = np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], axis=1)
+    p = p + 0.1 * np.sqrt(4 * np.pi / n) * rng.standard_normal(p.shape)
+    tree = trees.build_tree(0.5 + 0.45 * p, maxvalues=128, root_center=[0.5] * 3, root_halfsize=0.5)
+    k = 8 * np.pi * 0.45
+    core = methods.interpolation_core(tree, methods.helmholtz(k), 6, near="none", symmetry=True,
+                                      precision=precision)
+    assembly.near_blocks_device(core, "helmholtz", wavenumber=k, device=device)
+    return h2, core
+
+
+def sphere_arm(args):
+    """Dense (Chebyshev) far field on the sphere configuration's shape: FP64 and FP32 forms, 32
+    complex right-hand sides per matvec, forward/adjoint alternating (device timing)."""
+    import copy
+
+    import torch
+
+    device = "cuda:0"
+    h2, core = sphere_core(args.n, device)
+    n = core.trial.npoints
+    stream = torch.cuda.current_stream(device)
+    x = torch.randn((32, n), dtype=torch.complex128, device=device).t()
+    out = {}
+    ref = None
+    for prec in ("fp64", "fp32"):
+        c = copy.copy(core)
+        c.precision = prec
+        ws = h2.H2Workspace(c, max_nrhs=32)
+        y = torch.zeros((32, n), dtype=torch.complex128, device=device).t()
+        views = [ws, h2.adjoint(ws)]
+        per, tot = time_loop(torch, lambda i: h2.mul_(y, views[i % 2], x, stream=stream.cuda_stream),
+                             args.steps, args.warmup, stream)
+        h2.mul_(y, ws, x, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        if ref is None:
+            ref = y.clone()
+        out[prec] = {"rhs_per_s": 32 * args.steps / (tot * 1e-3), "ms_per_step": tot / args.steps,
+                     "p50_ms": pct(per, 50), "p99_ms": pct(per, 99),
+                     "rel_err_vs_fp64": float(((y - ref).norm(dim=0) / ref.norm(dim=0)).max())}
+        ws.close()
+        ws.dcore.close()
+    print(json.dumps({
+        "metric": METRIC, "value": out["fp32"]["rhs_per_s"], "unit": "RHS/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": out["fp32"]["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 far / c128 near", "data": "synthetic (seeded sphere)",
+        "config": {"workload": f"sphere-helmholtz-cheb6-N{n}", "rhs_per_step": 32, "modes": "forward/adjoint",
+                   "far_pairs": int(core.plans.far.shape[0]), "near_entries": int(core.near_device.numel()),
+                   "l2": "near blocks larger than L2; no flush"},
+        "fp64": out["fp64"], "fp32": out["fp32"]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -526,6 +591,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving leg length (0: skip)")
     ap.add_argument("--no-matrix-free", dest="matrix_free", action="store_false",
                     help="skip the matrix-free near-field forms")
+    ap.add_argument("--sphere", action="store_true",
+                    help="time the sphere configuration's shape at --n points instead (dense far field)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -533,6 +600,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.sphere:
+        sphere_arm(args)
         return
     if world > 1:
         import datetime
