@@ -212,8 +212,12 @@ h2b_status validate_side(const h2b_map_desc &d, const h2b_side_desc &s, const h2
         }
     const int nval = s.value_ptr[s.nnodes];
     if (nval > 0 && !s.value) return fail(H2B_ERR_INVALID, "%s: missing values", name);
-    for (int k = 0; k < nval; ++k)
+    if (nval > s.ndofs) return fail(H2B_ERR_INVALID, "%s: more dof ids than dofs", name);
+    std::vector<uint8_t> owned(s.ndofs, 0);  // every dof belongs to one leaf at most
+    for (int k = 0; k < nval; ++k) {
         if (s.value[k] < 0 || s.value[k] >= s.ndofs) return fail(H2B_ERR_INVALID, "%s: dof id out of range", name);
+        if (owned[s.value[k]]++) return fail(H2B_ERR_INVALID, "%s: dof %d in two leaves", name, s.value[k]);
+    }
 
     // aggregation plan
     std::vector<uint8_t> inagg(s.nnodes, 0);
@@ -695,6 +699,33 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
         std::vector<int> fill(ptr.begin(), ptr.end() - 1);
         for (int b = 0; b < nb; ++b) blk[fill[slot[key[b]]]++] = b;
     };
+    // work units of every group in block order: {first input value, columns (<= 32), element
+    // offset of the chunk's first column in the padded layout (low, high 32 bits)}
+    auto units = [&](NearOp &op, const h2b_side_desc &out, const h2b_side_desc &in, const std::vector<int> &key_in,
+                     const std::vector<int> &leaf, const std::vector<int> &ptr, const std::vector<int> &blk,
+                     const std::vector<int64_t> &off) -> h2b_status {
+        std::vector<int> uptr(leaf.size() + 1, 0);
+        std::vector<int4> ulist;
+        for (size_t g = 0; g < leaf.size(); ++g) {
+            const int64_t ld = near_padded_ld(cplx, nv(out, leaf[g]));
+            for (int bb = ptr[g]; bb < ptr[g + 1]; ++bb) {
+                const int b = blk[bb], c0 = in.value_ptr[key_in[b]], nc = nv(in, key_in[b]);
+                for (int j0 = 0; j0 < nc; j0 += 32) {
+                    const int64_t o = off[b] + j0 * ld;
+                    ulist.push_back(make_int4(c0 + j0, std::min(32, nc - j0), (int)(uint32_t)o, (int)(o >> 32)));
+                }
+            }
+            uptr[g + 1] = (int)ulist.size();
+        }
+        if (ulist.empty()) ulist.push_back(make_int4(0, 0, 0, 0));
+        int *pp;
+        int4 *pu;
+        CUDA_TRY(c->upload(&pp, uptr.data(), uptr.size()));
+        CUDA_TRY(c->upload(&pu, ulist.data(), ulist.size()));
+        op.unit_ptr = pp;
+        op.unit = pu;
+        return H2B_OK;
+    };
     int *p;
     int64_t *q;
     int *d_row, *d_col;
@@ -755,6 +786,7 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
         CUDA_TRY(c->upload(&p, blk.data(), blk.size())); op.grp_blk = p;
         op.blk_in = d_col;
         CUDA_TRY(c->upload(&q, fwd_off.data(), fwd_off.size())); op.blk_off = q;
+        if (h2b_status us = units(op, d.test, d.trial, blk_col, leaf, ptr, blk, fwd_off)) return us;
         unsigned char *data;
         CUDA_TRY(c->alloc(&data, (size_t)std::max<int64_t>(fwd_len, 2) * vb));
         op.data = data;
@@ -809,6 +841,7 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
         CUDA_TRY(c->upload(&p, blk.data(), blk.size())); op.grp_blk = p;
         op.blk_in = d_row;
         CUDA_TRY(c->upload(&q, tr_off.data(), tr_off.size())); op.blk_off = q;
+        if (h2b_status us = units(op, d.trial, d.test, blk_row, leaf, ptr, blk, tr_off)) return us;
         unsigned char *data;
         CUDA_TRY(c->alloc(&data, (size_t)std::max<int64_t>(tr_len, 2) * vb));
         op.data = data;

@@ -116,6 +116,11 @@ struct NearOp {
     const int *grp_blk = nullptr;   // block ids
     const int *blk_in = nullptr;    // input leaf of each block
     const int64_t *blk_off = nullptr;
+    // (block, 32-column chunk) work units of each group in block order (stored blocks only):
+    // {first input value, columns (<= 32), element offset of the chunk's first column (low, high
+    // 32 bits)}; one independent 16-byte load per unit instead of a chain block -> leaf -> values
+    const int *unit_ptr = nullptr;  // [ngroups+1]
+    const int4 *unit = nullptr;
     const void *data = nullptr;     // V
 };
 

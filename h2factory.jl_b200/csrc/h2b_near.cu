@@ -81,7 +81,7 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
     const int g = blockIdx.x;
     const int leaf = op.grp_leaf[g];
     const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
-    const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
+    const int u0 = op.unit_ptr[g], u1 = op.unit_ptr[g + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     V *xs = reinterpret_cast<V *>(smem_raw) + warp * 32 * R;                 // this warp's x chunk
     V *part = reinterpret_cast<V *>(smem_raw) + NEAR_WARPS * 32 * R;         // partial rows
@@ -104,25 +104,19 @@ near_rows_kernel(NearOp op, DSide outs, DSide ins, bool cjg, int r0, int rc, con
 #pragma unroll
                 for (int q = 0; q < R; ++q) acc[c][k][q] = V{};
         // work units are (block, 32-column chunk) pairs, dealt round-robin to the warps
-        int unit = 0;
-        for (int bb = b0; bb < b1; ++bb) {
-            const int blk = op.grp_blk[bb];
-            const int inl = op.blk_in[blk];
-            const int c0 = ins.value_ptr[inl], nc = ins.value_ptr[inl + 1] - c0;
-            const V *B = D + op.blk_off[blk] + i0;
-            for (int j0 = 0; j0 < nc; j0 += 32, ++unit) {
-                if (unit % NEAR_WARPS != warp) continue;
+        {
+            for (int un = u0 + warp; un < u1; un += NEAR_WARPS) {
+                const int4 ue = op.unit[un];
+                const int jn = ue.y;
                 __syncwarp();
                 {
-                    const int jl = j0 + lane;
-                    const int dof = jl < nc ? ins.value[c0 + jl] : 0;
+                    const int dof = lane < jn ? ins.value[ue.x + lane] : 0;
 #pragma unroll
                     for (int q = 0; q < R; ++q)
-                        xs[lane * R + q] = (jl < nc && q < rc) ? x[(int64_t)(r0 + q) * ldx + dof] : V{};
+                        xs[lane * R + q] = (lane < jn && q < rc) ? x[(int64_t)(r0 + q) * ldx + dof] : V{};
                 }
                 __syncwarp();
-                const int jn = min(32, nc - j0);
-                const V *Bj = B + (int64_t)j0 * ld;
+                const V *Bj = D + (((int64_t)ue.w << 32) | (uint32_t)ue.z) + i0;
                 int jj = 0;
                 for (; jj + UB <= jn; jj += UB) {
                     V bv[UB][MP][RPL];  // UB columns in flight before any use
@@ -255,43 +249,28 @@ near_rows_mma_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const dou
     const int g = blockIdx.x;
     const int leaf = op.grp_leaf[g];
     const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
-    const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
+    const int u0 = op.unit_ptr[g], u1 = op.unit_ptr[g + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g4 = lane >> 2, t4 = lane & 3;
     const int half = warp >> 2, wq = warp & 3;
     double *ring = reinterpret_cast<double *>(smem_raw) + (size_t)warp * MST * SS;
     double *part = reinterpret_cast<double *>(smem_raw);  // [8 warps][32 rows][R], after the units
     const double *D = static_cast<const double *>(op.data);
-    const int ld = nr + (nr & 1);
     for (int p0 = 0; p0 < nr; p0 += 64) {
         const int rows0 = p0 + 32 * half;
         const bool active = rows0 < nr;
         const int rpairs = active ? (min(32, nr - rows0) + 1) / 2 : 0;  // 16-byte row pairs
-        // producer cursor: block pb, first column pj of the stage, ubase = unit index of the
-        // block's first 32-column unit; a stage belongs to this warp when its unit does
-        auto ncols = [&](int bb) {
-            const int inl = op.blk_in[op.grp_blk[bb]];
-            return ins.value_ptr[inl + 1] - ins.value_ptr[inl];
-        };
-        int pb = b0, pj = -MCOLS, ubase = 0;
-        int pnc = pb < b1 ? ncols(pb) : 0;
-        auto next_stage = [&]() {
-            while (true) {
-                pj += MCOLS;
-                while (pb < b1 && pj >= pnc) {
-                    ubase += (pnc + 31) / 32;
-                    ++pb;
-                    pj = 0;
-                    pnc = pb < b1 ? ncols(pb) : 0;
-                }
-                if (pb >= b1 || (ubase + pj / 32) % 4 == wq) return;
-            }
-        };
-        auto issue = [&](int slot) {
-            if (active && pb < b1) {
-                const int blk = op.grp_blk[pb];
-                const int c0 = ins.value_ptr[op.blk_in[blk]], nc = pnc;
-                const double *B = D + op.blk_off[blk] + rows0;
+        const int ld = nr + (nr & 1);
+        // producer cursor: this warp's unit pu (units wq, wq + 4, ... of the group), its entry ue,
+        // the next one un (loaded a unit ahead), and the first column pj of the next stage
+        int pu = active ? u0 + wq : u1, pj = 0;
+        int4 ue = pu < u1 ? op.unit[pu] : make_int4(0, 0, 0, 0);
+        int4 un = pu + 4 < u1 ? op.unit[pu + 4] : ue;
+        auto issue = [&](int slot) -> int {  // one commit group per call; 1 if it holds a stage
+            int got = 0;
+            if (pu < u1) {
+                const int c0 = ue.x, nc = ue.y;
+                const double *B = D + (((int64_t)ue.w << 32) | (uint32_t)ue.z) + rows0;
                 double *sa = ring + slot * SS, *sx = sa + SA;
                 // slab: MCOLS columns x 16 row pairs, 16-byte pieces
                 for (int c = lane; c < MCOLS * 16; c += 32) {
@@ -305,32 +284,29 @@ near_rows_mma_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const dou
                     const bool ok = pj + col < nc;
                     cp16(sx + col * XS + q, ok ? xp + (int64_t)(c0 + pj + col) * R + q : xp, ok);
                 }
-                next_stage();
+                got = 1;
+                pj += MCOLS;
+                if (pj >= nc) {
+                    pj = 0;
+                    pu += 4;
+                    ue = un;
+                    if (pu + 4 < u1) un = op.unit[pu + 4];
+                }
             }
             cp_commit();
+            return got;
         };
         double acc[4][NT][2];
 #pragma unroll
         for (int t = 0; t < 4; ++t)
 #pragma unroll
             for (int u = 0; u < NT; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
-        // number of stages this warp consumes
-        int nstages = 0;
-        if (active) {
-            int u = 0;
-            for (int bb = b0; bb < b1; ++bb) {
-                const int inl = op.blk_in[op.grp_blk[bb]];
-                const int nc = ins.value_ptr[inl + 1] - ins.value_ptr[inl];
-                for (int j0 = 0; j0 < nc; j0 += 32, ++u)
-                    if (u % 4 == wq) nstages += (min(32, nc - j0) + MCOLS - 1) / MCOLS;
-            }
-        }
-        if (active) next_stage();
+        int nstages = 0;  // stages issued so far; the loop below runs until it has consumed them all
 #pragma unroll
-        for (int s2 = 0; s2 < MST - 1; ++s2) issue(s2);
+        for (int s2 = 0; s2 < MST - 1; ++s2) nstages += issue(s2);
         int slot = 0;
         for (int st = 0; st < nstages; ++st) {
-            issue((slot + MST - 1) % MST);
+            nstages += issue((slot + MST - 1) % MST);
             cp_wait<MST - 1>();
             __syncwarp();
             const double *sa = ring + slot * SS + 4 * g4, *sx = ring + slot * SS + SA + g4;

@@ -79,6 +79,7 @@ def create(lib, desc):
     (lambda d, k: setattr(d, "ncomp", 0), "ncomp"),
     (lambda d, k: setattr(d, "coupling_kind", 9), "coupling kind"),
     (lambda d, k: k.bad_value(d), "dof id"),
+    (lambda d, k: k.dup_value(d), "in two leaves"),
     (lambda d, k: k.bad_coupling(d), "coupling index"),
     (lambda d, k: k.bad_near(d), "near block"),
     (lambda d, k: k.bad_stage_order(d), "aggregation"),
@@ -96,6 +97,12 @@ def test_malformed_maps_are_rejected(lib, small_core, mutate, msg):
             n = d.test.value_ptr[d.test.nnodes]
             arr = np.ctypeslib.as_array(d.test.value, shape=(n,))
             arr[3] = d.test.ndofs + 5
+
+        @staticmethod
+        def dup_value(d):
+            n = d.test.value_ptr[d.test.nnodes]
+            arr = np.ctypeslib.as_array(d.test.value, shape=(n,))
+            arr[3] = arr[n - 1]
 
         @staticmethod
         def bad_coupling(d):
