@@ -748,10 +748,10 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
             groups(side == 0 ? d.test : d.trial, side == 0 ? blk_row : blk_col, leaf, ptr, blk);
             NearOp &op = side == 0 ? dn.fwd : dn.tr;
             CUDA_TRY(c->upload(&p, leaf.data(), leaf.size())); op.grp_leaf = p;
-            CUDA_TRY(c->upload(&p, ptr.data(), ptr.size())); op.grp_ptr = p;
-            CUDA_TRY(c->upload(&p, blk.data(), blk.size())); op.grp_blk = p;
-            op.blk_in = side == 0 ? d_col : d_row;
             op.ngroups = (int)leaf.size();
+            if (h2b_status us = units(op, side == 0 ? d.test : d.trial, side == 0 ? d.trial : d.test,
+                                      side == 0 ? blk_col : blk_row, leaf, ptr, blk, side == 0 ? fwd_off : tr_off))
+                return us;
         }
         dn.symmetric = false;
         CUDA_TRY(cudaDeviceSynchronize());
@@ -782,9 +782,6 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
         groups(d.test, blk_row, leaf, ptr, blk);
         NearOp &op = c->dnear.fwd;
         CUDA_TRY(c->upload(&p, leaf.data(), leaf.size())); op.grp_leaf = p;
-        CUDA_TRY(c->upload(&p, ptr.data(), ptr.size())); op.grp_ptr = p;
-        CUDA_TRY(c->upload(&p, blk.data(), blk.size())); op.grp_blk = p;
-        op.blk_in = d_col;
         CUDA_TRY(c->upload(&q, fwd_off.data(), fwd_off.size())); op.blk_off = q;
         if (h2b_status us = units(op, d.test, d.trial, blk_col, leaf, ptr, blk, fwd_off)) return us;
         unsigned char *data;
@@ -837,9 +834,6 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
         groups(d.trial, blk_col, leaf, ptr, blk);
         NearOp &op = c->dnear.tr;
         CUDA_TRY(c->upload(&p, leaf.data(), leaf.size())); op.grp_leaf = p;
-        CUDA_TRY(c->upload(&p, ptr.data(), ptr.size())); op.grp_ptr = p;
-        CUDA_TRY(c->upload(&p, blk.data(), blk.size())); op.grp_blk = p;
-        op.blk_in = d_row;
         CUDA_TRY(c->upload(&q, tr_off.data(), tr_off.size())); op.blk_off = q;
         if (h2b_status us = units(op, d.trial, d.test, blk_row, leaf, ptr, blk, tr_off)) return us;
         unsigned char *data;

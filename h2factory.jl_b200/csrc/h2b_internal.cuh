@@ -112,13 +112,11 @@ struct DMap {
 struct NearOp {
     int ngroups = 0;
     const int *grp_leaf = nullptr;  // [ngroups] output leaf (every output leaf has a group)
-    const int *grp_ptr = nullptr;   // [ngroups+1]
-    const int *grp_blk = nullptr;   // block ids
-    const int *blk_in = nullptr;    // input leaf of each block
-    const int64_t *blk_off = nullptr;
-    // (block, 32-column chunk) work units of each group in block order (stored blocks only):
-    // {first input value, columns (<= 32), element offset of the chunk's first column (low, high
-    // 32 bits)}; one independent 16-byte load per unit instead of a chain block -> leaf -> values
+    const int64_t *blk_off = nullptr;  // per block id: element offset in `data`
+    // (block, 32-column chunk) work units of each group in block order: {first input value,
+    // columns (<= 32), element offset of the chunk's first column in `data` (low, high 32 bits;
+    // unused by the matrix-free kernels)}; one independent 16-byte load per unit instead of a
+    // chain block -> input leaf -> values
     const int *unit_ptr = nullptr;  // [ngroups+1]
     const int4 *unit = nullptr;
     const void *data = nullptr;     // V

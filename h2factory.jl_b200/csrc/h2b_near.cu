@@ -409,7 +409,7 @@ near_free_kernel(NearOp op, DSide outs, DSide ins, const double *__restrict__ po
     const int g = blockIdx.x;
     const int leaf = op.grp_leaf[g];
     const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
-    const int b0 = op.grp_ptr[g], b1 = op.grp_ptr[g + 1];
+    const int u0 = op.unit_ptr[g], u1 = op.unit_ptr[g + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     V *xs = reinterpret_cast<V *>(smem_raw) + warp * 32 * R;             // this warp's x chunk
     double *qs = reinterpret_cast<double *>(reinterpret_cast<V *>(smem_raw) + NEAR_WARPS * 32 * R) +
@@ -432,26 +432,20 @@ near_free_kernel(NearOp op, DSide outs, DSide ins, const double *__restrict__ po
 #pragma unroll
             for (int q = 0; q < R; ++q) acc[k][q] = V{};
         }
-        int unit = 0;
-        for (int bb = b0; bb < b1; ++bb) {
-            const int blk = op.grp_blk[bb];
-            const int inl = op.blk_in[blk];
-            const int c0 = ins.value_ptr[inl], nc = ins.value_ptr[inl + 1] - c0;
-            for (int j0 = 0; j0 < nc; j0 += 32, ++unit) {
-                if (unit % NEAR_WARPS != warp) continue;
+        {
+            for (int un = u0 + warp; un < u1; un += NEAR_WARPS) {
+                const int jn = op.unit[un].y, c0 = op.unit[un].x;
                 __syncwarp();
                 {
-                    const int jl = j0 + lane;
-                    const int64_t dof = jl < nc ? ins.value[c0 + jl] : 0;
+                    const int64_t dof = lane < jn ? ins.value[c0 + lane] : 0;
 #pragma unroll
                     for (int q = 0; q < R; ++q)
-                        xs[lane * R + q] = (jl < nc && q < rc) ? x[(int64_t)(r0 + q) * ldx + dof] : V{};
+                        xs[lane * R + q] = (lane < jn && q < rc) ? x[(int64_t)(r0 + q) * ldx + dof] : V{};
                     qs[3 * lane] = pin[3 * dof];
                     qs[3 * lane + 1] = pin[3 * dof + 1];
                     qs[3 * lane + 2] = pin[3 * dof + 2];
                 }
                 __syncwarp();
-                const int jn = min(32, nc - j0);
                 for (int jj = 0; jj < jn; ++jj) {
                     const double qx = qs[3 * jj], qy = qs[3 * jj + 1], qz = qs[3 * jj + 2];
                     V xv[R];
