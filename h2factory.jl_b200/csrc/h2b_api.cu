@@ -1015,6 +1015,19 @@ int32_t h2b_version(void) { return (1 << 16) | 0; }
 
 const char *h2b_last_error(void) { return g_err.c_str(); }
 
+h2b_status h2b_tensor_wait_timeouts(int32_t device, uint32_t *count) {
+    if (!count) return fail(H2B_ERR_INVALID, "null argument");
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(H2B_ERR_INVALID, "device %d not present", device);
+    DeviceGuard guard(device);
+    CUDA_TRY(cudaDeviceSynchronize());
+    unsigned v = 0;
+    CUDA_TRY(read_umma_timeouts(&v));
+    *count = v;
+    return H2B_OK;
+}
+
 h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **out) {
     if (!desc || !out) return fail(H2B_ERR_INVALID, "null argument");
     *out = nullptr;

@@ -175,6 +175,13 @@ cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &rec
 cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const DSide &s,
                                 const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
                                 int maxtsize, int maxaxis, cudaStream_t st);
+// Dense I2O of the FP32 form on the tcgen05 tensor cores (h2b_umma.cu): taken when the coupling
+// storage is dense and the right-hand sides fill an MMA of N >= 16 FP32 columns.
+bool i2o_umma_eligible(bool cplx, int precision, const DMap &m, int nq);
+cudaError_t launch_i2o_umma(bool cplx, const DMap &m, const DSide &recv, const DSide &src, const int *nodes,
+                            int nnodes, const FarArgs &fa, int maxcoef, cudaStream_t st);
+// mbarrier waits of the tensor-core kernels that gave up on the current device (0 in a healthy run)
+cudaError_t read_umma_timeouts(unsigned *count);
 cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const DSide &recv,
                                 const SibGroups &g, int maxslen, const FarArgs &fa, cudaStream_t st);
 cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const DSide &s,

@@ -1270,6 +1270,8 @@ cudaError_t launch_i2o(bool cplx, int precision, const DMap &m, const DSide &rec
                        const DSide &src, const int *nodes, int nnodes, const FarArgs &fa,
                        int maxcoef, int maxtsize, int maxhalf, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
+    if (i2o_umma_eligible(cplx, precision, m, m.ncomp * fa.nrhs))
+        return launch_i2o_umma(cplx, m, recv, src, nodes, nnodes, fa, maxcoef, st);
     // Toeplitz: one thread per stored frequency (half spectra hold (n1/2 + 1) * n2 * n3 of them);
     // dense: the tile product's 256 threads
     const bool toep = m.coupling_kind == H2B_COUPLING_TOEPLITZ;

@@ -216,6 +216,13 @@ int32_t h2b_version(void);
 /* Text of the last failure on the calling thread. */
 const char *h2b_last_error(void);
 
+/* Number of waits of the library's tensor-core kernels that gave up on `device` since the library
+ * was loaded. Every mbarrier wait inside a kernel is bounded; a wait that runs out adds one here,
+ * and its CTA stops, frees its tensor memory and leaves its output tile unwritten. 0 in a healthy
+ * run; read it after a product to rule out such a tile. Waits for the device's queued work.
+ * No counterpart in the reference: its CPU map has no device-side waits. */
+h2b_status h2b_tensor_wait_timeouts(int32_t device, uint32_t *count);
+
 /* Validate `desc`, copy it to `device` and build the read-only core: the CUDA equivalent of
  * building an AbstractH2Core (src/maps/core.jl:17-33). The caller keeps its host arrays. */
 h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **out);
