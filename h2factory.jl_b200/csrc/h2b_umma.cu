@@ -6,23 +6,25 @@
 // of i2oprotocol.jl:87-92). For one receiver this is one GEMM whose K dimension runs over the
 // concatenated pairs: D[nc x nq] = [op(B_1) op(B_2) ...] [m_1; m_2; ...].
 //
-// One CTA per (receiver, 128-row tile of its coefficients, tile of right-hand sides). All 256
-// threads stage 32-wide K chunks of both operands from global memory (L2-resident couplings and
-// moments) into shared memory in the canonical no-swizzle K-major layout, splitting every FP32
-// value into a TF32 high part and a TF32 remainder; one thread issues per 8-wide k step the three
-// products hi*hi + hi*lo + lo*hi (the lo*lo term is below FP32 rounding) into an FP32 accumulator
-// in tensor memory; a commit to an mbarrier per stage releases the buffer, so staging chunk c + 1
-// overlaps the products of chunk c. Accumulators live for 4 chunks (48 MMAs) only: two alternate,
-// and each finished one is added into an FP64 sum kept in tensor memory, because every MMA rounds
-// its accumulator toward zero (one accumulator through a whole interaction list, ~30,000 MMAs,
-// measured 1e-4 relative error; segments keep it near FP32 rounding). The epilogue reads the sums
-// with tcgen05.ld and stores the FP32 moments.
+// One CTA per (receiver, 128-row tile of its coefficients, tile of right-hand sides), two CTAs per
+// SM. The K dimension streams in chunks of 16 FP32 values: every thread copies its share of chunk
+// c + 3 from global memory (L2-resident couplings and moments) into a 4-stage ring of raw shared
+// buffers with cp.async (gathers and zero fill included), so three chunks are in flight without
+// registers; a split pass turns raw chunk c into the canonical no-swizzle K-major layout of the
+// tensor cores, each FP32 value as a TF32 high part and a TF32 remainder; one thread issues per
+// 8-wide k step the three products hi*hi + hi*lo + lo*hi (the lo*lo term is below FP32 rounding)
+// into an FP32 accumulator in tensor memory, and a commit to an mbarrier per split buffer releases
+// it, so splitting chunk c + 1 overlaps the products of chunk c. Accumulators live for 8 chunks (48
+// MMAs) only: two alternate, and each finished one is added into an FP64 sum kept in tensor memory,
+// because every MMA rounds its accumulator toward zero (one accumulator through a whole interaction
+// list, ~30,000 MMAs, measured 1e-4 relative error; segments keep it near FP32 rounding). The
+// epilogue reads the sums with tcgen05.ld and stores the FP32 moments.
 //
 // Complex maps run as real GEMMs: with B = Br + i Bi and m = mr + i mi,
 //   [Re l | Im l] = [Br Bi] (interleaved along k) x [[mr, mi]; [-mi, mr]] (interleaved rows),
 // so the coupling's interleaved (re, im) storage is the A operand as it lies in memory and each
-// moment value feeds two B rows. Adjoint maps conjugate B while staging; symmetry-reduced
-// couplings apply their row / column permutations in the staging loads.
+// moment value feeds two B rows. Adjoint maps conjugate B in the split pass; symmetry-reduced
+// couplings apply their row / column permutations in the copy addresses.
 //
 // Every wait on an mbarrier is bounded: a wait that gives up counts itself in a device counter
 // (h2b_tensor_wait_timeouts), the CTA stops issuing, frees its tensor memory and returns.
@@ -34,15 +36,17 @@ namespace h2b {
 namespace {
 
 constexpr int UM_M = 128;        // output rows per tile = tensor-memory lanes
-constexpr int UM_KC = 32;        // FP32 K values per staged chunk: 8 groups of 16 bytes per row
+constexpr int UM_KC = 16;        // FP32 K values per chunk: 4 groups of 16 bytes per row
+constexpr int UM_KG = UM_KC / 4;
 constexpr int UM_THREADS = 256;
-constexpr int UM_AGRP = UM_M * (UM_KC / 4) / UM_THREADS;  // A groups per thread per chunk (4)
-constexpr int UM_BGRP = 2;                                // B groups per thread per chunk, at most
 constexpr int UM_NT_MAX = 64;    // MMA N (FP32 accumulator columns) per tile, at most
-constexpr int UM_SEG = 4;        // chunks (48 MMAs) per accumulation segment
-constexpr uint32_t UM_LBO = 128;     // bytes between the two 16-byte K halves of an 8-wide k step
-constexpr uint32_t UM_SBO = 1024;    // bytes between 8-row groups (8 groups of 128 bytes along K)
-constexpr uint32_t UM_AHALF = UM_M * UM_KC * 4;  // bytes of one A split part per stage (16 KB)
+constexpr int UM_SEG = 8;        // chunks (48 MMAs) per accumulation segment
+constexpr int UM_RS = 4;         // raw stages: chunks c + 1 .. c + 3 in flight while c is split
+constexpr uint32_t UM_LBO = 128;           // bytes between the two 16-byte K halves of a k step
+constexpr uint32_t UM_SBO = UM_KG * 128;   // bytes between 8-row groups (4 groups of 128 bytes)
+constexpr uint32_t UM_AHALF = UM_M * UM_KC * 4;  // bytes of one A split part (8 KB)
+constexpr uint32_t UM_RAWROW = UM_KC * 4 + 16;   // raw row layout: 64 bytes + 16 of padding
+constexpr uint32_t UM_RAWA = UM_M * UM_RAWROW;   // raw A bytes (>= the column layouts' 8,448)
 constexpr unsigned UM_SPIN = 1u << 22;           // try_wait attempts before a wait gives up
 
 __device__ unsigned int g_umma_timeouts = 0;
@@ -69,7 +73,7 @@ __device__ __forceinline__ uint32_t tf32_idesc(int mrows, int ncols) {
            ((uint32_t)(mrows >> 4) << 24);
 }
 
-// byte offset of the 16-byte group (row, kg) in a no-swizzle K-major tile of 32-wide rows
+// byte offset of the 16-byte group (row, kg) in a no-swizzle K-major tile of 16-wide rows
 __device__ __forceinline__ uint32_t goff(int row, int kg) {
     return (uint32_t)(row >> 3) * UM_SBO + (uint32_t)kg * UM_LBO + (uint32_t)(row & 7) * 16u;
 }
@@ -152,6 +156,17 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
     for (int u = 0; u < 8; ++u) v[u] = __uint_as_float(r[u]);
 }
 
+// element copy global -> shared; src_bytes 0 writes zeros (src is then not read)
+template <int EB>
+__device__ __forceinline__ void cp_elem(uint32_t dst, const void *src, bool ok) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(EB), "r"(ok ? EB : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <class T> struct UmScalar;
 template <> struct UmScalar<float> {
     static constexpr int W = 1;  // FP32 values per element
@@ -179,9 +194,12 @@ __global__ void __launch_bounds__(UM_THREADS)
 i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mode, int nrhs, int qt_max,
                 const T *__restrict__ am, T *__restrict__ dm) {
     constexpr int W = UmScalar<T>::W;
-    extern __shared__ __align__(1024) unsigned char um_smem[];
+    constexpr int EB = sizeof(T);        // bytes per element (4 real, 8 complex)
+    constexpr int KQ = UM_KC / W;        // elements along k per chunk
+    extern __shared__ __align__(128) unsigned char um_smem[];
     __shared__ uint64_t bar[2];
     __shared__ uint32_t tmem_slot;
+    __shared__ int nchunks_s;
 
     const int node = nodes[blockIdx.x];
     const int nc = um_ncoef(r, r.level[node]);
@@ -192,9 +210,11 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     const int mt = min(UM_M, nc - m0);
     const int qt = min(qt_max, nq - q0);
     const int nt = ((W * qt + 15) / 16) * 16;                 // MMA N of this tile
-    const int ntmax = ((W * qt_max + 15) / 16) * 16;          // B rows the stage holds
-    const int lb = W == 1 ? nt : ((qt + 7) / 8) * 8;          // B rows loaded per chunk
-    const uint32_t stage_bytes = 2 * UM_AHALF + 2u * (uint32_t)ntmax * 128u;
+    const int ntmax = ((W * qt_max + 15) / 16) * 16;          // B rows a split buffer holds
+    const int lb = W == 1 ? nt : ((qt + 7) / 8) * 8;          // B rows copied per chunk
+    const int lbmax = W == 1 ? ntmax : ((qt_max + 7) / 8) * 8;
+    const uint32_t split_bytes = 2 * UM_AHALF + 2u * (uint32_t)ntmax * (UM_KC * 4);
+    const uint32_t raw_bytes = UM_RAWA + (uint32_t)lbmax * UM_RAWROW;
     const int p0 = r.i2o_ptr[node], p1 = r.i2o_ptr[node + 1];
     T *out = dm + r.mom_off[node] * nrhs;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -218,6 +238,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[0])) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        nchunks_s = 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -244,111 +265,134 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
         }
         return u;
     };
-    // op(B)[i, k] of the pair (i a row of the tile, k a source coefficient)
-    auto bval = [&](const UmPair<T> &u, int i, int k) -> T {
-        const int ii = u.rowmap ? u.rowmap[i] : i;
-        const T b = fwd ? u.B[ii + (int64_t)k * nc] : u.B[k + (int64_t)ii * u.snc];
-        return cj(b, adj);
-    };
-    auto xval = [&](const UmPair<T> &u, int q, int k) -> T {
-        return u.X[(int64_t)q * u.snc + (u.xmap ? u.xmap[k] : k)];
-    };
-    // the 16-byte groups of thread tid: A rows along i for forward blocks (consecutive lanes read
-    // consecutive elements of a column), 8 rows x 4 groups per warp otherwise (each row's 64 bytes
-    // read by 4 lanes); B always the latter. Both write shared memory without bank conflicts.
-    auto amap = [&](int g, int &row, int &kg) {
+    {  // chunks of the whole interaction list
+        int mine = 0;
+        for (int p = p0 + tid; p < p1; p += UM_THREADS) mine += (W * um_ncoef(t, t.level[r.i2o_src[p]]) + UM_KC - 1) / UM_KC;
+        if (mine) atomicAdd(&nchunks_s, mine);
+        __syncthreads();
+    }
+    const int C = nchunks_s;
+
+    // Copy mappings. A, forward blocks (column-major, rows contiguous): thread = one tile row,
+    // consecutive lanes consecutive rows, raw layout [k][row]. A, transposed blocks (rows
+    // contiguous along k) and B (moment columns contiguous along k): a warp covers 8 rows x 4
+    // consecutive k, raw layout [row][k] with 80-byte rows. The tile rows a thread copies are
+    // fixed, so a permuted block's row map is read once per pair.
+    const int arow_f = tid & (UM_M - 1);                       // forward: the thread's row
+    const int arow_t0 = (warp & 7) * 8 + (lane & 7);           // transposed: rows arow_t0, + 64
+    const uint32_t colstride = UM_M * EB + 16;                 // raw column layout: bytes per k
+    int pp = p0, pk = 0, issued = 0;  // copy cursor: pair, chunk within it, chunks issued
+    UmPair<T> pu = pair_at(p0);
+    int hrow[2];
+    auto load_rows = [&]() {
         if (fwd) {
-            row = g & (UM_M - 1);
-            kg = g >> 7;
+            hrow[0] = arow_f < mt ? (pu.rowmap ? pu.rowmap[m0 + arow_f] : m0 + arow_f) : 0;
+            hrow[1] = 0;
         } else {
-            const int w = g >> 5, l = g & 31;
-            row = (w & 15) * 8 + (l & 7);
-            kg = (w >> 4) * 4 + (l >> 3);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int rr = arow_t0 + 64 * h;
+                hrow[h] = rr < mt ? (pu.rowmap ? pu.rowmap[m0 + rr] : m0 + rr) : 0;
+            }
         }
     };
-    auto bmap = [&](int g, int &row, int &kg) {
-        const int w = g >> 5, l = g & 31, nrb = lb >> 3;
-        row = (w % nrb) * 8 + (l & 7);
-        kg = (w / nrb) * 4 + (l >> 3);
+    load_rows();
+    const uint32_t smem0 = su32(um_smem);
+    const uint32_t raw0 = smem0 + 2 * split_bytes;
+    auto issue = [&]() {  // copies of the next chunk into raw stage (issued % UM_RS); one group
+        if (issued < C) {
+            const uint32_t ra = raw0 + (uint32_t)(issued % UM_RS) * raw_bytes, rb = ra + UM_RAWA;
+            const int kq0 = pk * KQ;
+            if (fwd) {
+#pragma unroll
+                for (int j = 0; j < KQ / 2; ++j) {
+                    const int kq = (tid >> 7) + 2 * j, k = kq0 + kq;
+                    const bool ok = arow_f < mt && k < pu.snc;
+                    cp_elem<EB>(ra + (uint32_t)kq * colstride + (uint32_t)arow_f * EB,
+                                ok ? pu.B + hrow[0] + (int64_t)k * nc : pu.B, ok);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < KQ / 2; ++j) {
+                    const int row = arow_t0 + 64 * (j & 1), kq = (j >> 1) * 4 + (lane >> 3), k = kq0 + kq;
+                    const bool ok = row < mt && k < pu.snc;
+                    cp_elem<EB>(ra + (uint32_t)row * UM_RAWROW + (uint32_t)kq * EB,
+                                ok ? pu.B + k + (int64_t)hrow[j & 1] * pu.snc : pu.B, ok);
+                }
+            }
+            const int nrb = lb >> 3;
+            for (int e = tid; e < lb * KQ; e += UM_THREADS) {
+                const int w = e >> 5, l = e & 31;
+                const int q = (w % nrb) * 8 + (l & 7), kq = (w / nrb) * 4 + (l >> 3), k = kq0 + kq;
+                const bool ok = q < qt && k < pu.snc;
+                const T *src = pu.X;
+                if (ok) src = pu.X + (int64_t)q * pu.snc + (pu.xmap ? pu.xmap[k] : k);
+                cp_elem<EB>(rb + (uint32_t)q * UM_RAWROW + (uint32_t)kq * EB, src, ok);
+            }
+            ++issued;
+            if (++pk == pu.nk) {
+                pk = 0;
+                if (++pp < p1) {
+                    pu = pair_at(pp);
+                    load_rows();
+                }
+            }
+        }
+        cp_commit_group();
     };
-
-    float av[UM_AGRP][4], bv[UM_BGRP][4];
-    auto load_chunk = [&](const UmPair<T> &u, int kc) {
+    // raw chunk -> split buffer: TF32 hi / lo in the canonical layout (A conjugated for adjoint maps)
+    auto split = [&](uint32_t ra, uint32_t sbase) {
+        const uint32_t rb = ra + UM_RAWA;
+        const uint32_t ahi = sbase, alo = sbase + UM_AHALF;
+        const uint32_t bhi = sbase + 2 * UM_AHALF, blo = bhi + (uint32_t)ntmax * (UM_KC * 4);
 #pragma unroll
-        for (int j = 0; j < UM_AGRP; ++j) {
+        for (int j = 0; j < UM_M * UM_KG / UM_THREADS; ++j) {
+            const int g = tid + UM_THREADS * j;
             int row, kg;
-            amap(tid + UM_THREADS * j, row, kg);
-            const int kb = kc * UM_KC + kg * 4;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) av[j][e] = 0.f;
-            if (row < mt) {
+            float v[4];
+            if (fwd) {
+                row = g & (UM_M - 1);
+                kg = g >> 7;
                 if constexpr (W == 1) {
 #pragma unroll
                     for (int e = 0; e < 4; ++e)
-                        if (kb + e < u.snc) av[j][e] = bval(u, m0 + row, kb + e);
+                        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v[e]) : "r"(ra + (uint32_t)(4 * kg + e) * colstride + (uint32_t)row * 4));
                 } else {
 #pragma unroll
                     for (int e = 0; e < 2; ++e)
-                        if (kb / 2 + e < u.snc) {
-                            const T b = bval(u, m0 + row, kb / 2 + e);
-                            av[j][2 * e] = b.x;
-                            av[j][2 * e + 1] = b.y;
-                        }
+                        asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
+                                     : "=f"(v[2 * e]), "=f"(v[2 * e + 1])
+                                     : "r"(ra + (uint32_t)(2 * kg + e) * colstride + (uint32_t)row * 8));
                 }
+            } else {
+                const int w = g >> 5, l = g & 31;
+                row = (w & 15) * 8 + (l & 7);
+                kg = (w >> 4) * 4 + (l >> 3);
+                asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                             : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+                             : "r"(ra + (uint32_t)row * UM_RAWROW + (uint32_t)kg * 16));
             }
-        }
-#pragma unroll
-        for (int j = 0; j < UM_BGRP; ++j) {
-            const int g = tid + UM_THREADS * j;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) bv[j][e] = 0.f;
-            if (g < lb * 8) {
-                int row, kg;
-                bmap(g, row, kg);
-                const int kb = kc * UM_KC + kg * 4;
-                if (row < qt) {
-                    if constexpr (W == 1) {
-#pragma unroll
-                        for (int e = 0; e < 4; ++e)
-                            if (kb + e < u.snc) bv[j][e] = xval(u, row, kb + e);
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < 2; ++e)
-                            if (kb / 2 + e < u.snc) {
-                                const T x = xval(u, row, kb / 2 + e);
-                                bv[j][2 * e] = x.x;
-                                bv[j][2 * e + 1] = x.y;
-                            }
-                    }
-                }
+            if (W == 2 && adj) {
+                v[1] = -v[1];
+                v[3] = -v[3];
             }
-        }
-    };
-    auto store_chunk = [&](uint32_t sbase) {
-        const uint32_t ahi = sbase, alo = sbase + UM_AHALF;
-        const uint32_t bhi = sbase + 2 * UM_AHALF, blo = bhi + (uint32_t)ntmax * 128u;
-#pragma unroll
-        for (int j = 0; j < UM_AGRP; ++j) {
-            int row, kg;
-            amap(tid + UM_THREADS * j, row, kg);
             const uint32_t o = goff(row, kg);
-            st_split(ahi + o, alo + o, av[j][0], av[j][1], av[j][2], av[j][3]);
+            st_split(ahi + o, alo + o, v[0], v[1], v[2], v[3]);
         }
-#pragma unroll
-        for (int j = 0; j < UM_BGRP; ++j) {
-            const int g = tid + UM_THREADS * j;
-            if (g < lb * 8) {
-                int row, kg;
-                bmap(g, row, kg);
-                if constexpr (W == 1) {
-                    const uint32_t o = goff(row, kg);
-                    st_split(bhi + o, blo + o, bv[j][0], bv[j][1], bv[j][2], bv[j][3]);
-                } else if (row < qt) {
-                    // row q: (mr, -mi) per k feeds Re; row qt + q: (mi, mr) feeds Im
-                    const uint32_t o1 = goff(row, kg), o2 = goff(qt + row, kg);
-                    st_split(bhi + o1, blo + o1, bv[j][0], -bv[j][1], bv[j][2], -bv[j][3]);
-                    st_split(bhi + o2, blo + o2, bv[j][1], bv[j][0], bv[j][3], bv[j][2]);
-                }
+        for (int g = tid; g < lb * UM_KG; g += UM_THREADS) {
+            const int q = g >> 2, kg = g & 3;
+            float v[4];
+            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                         : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+                         : "r"(rb + (uint32_t)q * UM_RAWROW + (uint32_t)kg * 16));
+            if constexpr (W == 1) {
+                const uint32_t o = goff(q, kg);
+                st_split(bhi + o, blo + o, v[0], v[1], v[2], v[3]);
+            } else if (q < qt) {
+                // row q: (mr, -mi) per k feeds Re; row qt + q: (mi, mr) feeds Im
+                const uint32_t o1 = goff(q, kg), o2 = goff(qt + q, kg);
+                st_split(bhi + o1, blo + o1, v[0], -v[1], v[2], -v[3]);
+                st_split(bhi + o2, blo + o2, v[1], v[0], v[3], v[2]);
             }
         }
     };
@@ -379,16 +423,17 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     };
 
-    const uint32_t smem0 = su32(um_smem);
     const uint32_t idesc = tf32_idesc(UM_M, nt);
-    int p = p0, kc = 0, c = 0;
-    UmPair<T> cur = pair_at(p);
-    load_chunk(cur, kc);
+#pragma unroll
+    for (int s = 0; s < UM_RS - 1; ++s) issue();
+    int c = 0;
     bool bad = false;
-    for (;;) {
+    for (; c < C; ++c) {
         const int s = c & 1, g = c / UM_SEG, a = g & 1;
-        const uint32_t sbase = smem0 + (uint32_t)s * stage_bytes;
-        // the products of chunk c - 2 read this stage: wait for their commit
+        const uint32_t sbase = smem0 + (uint32_t)s * split_bytes;
+        cp_wait_group<UM_RS - 2>();  // this thread's copies of chunk c have landed
+        __syncthreads();             // everyone's have
+        // the products of chunk c - 2 read this split buffer: wait for their commit
         if (c >= 2 && !bad) bad = !mbar_wait(&bar[s], ((c - 2) >> 1) & 1);
         if (c % UM_SEG == 0 && g >= 2) {
             // segment g - 2 ended at chunk (g - 1) UM_SEG - 1 <= c - 2: complete; free its
@@ -398,14 +443,14 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             drain(a, g == 2);
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         }
-        if (!bad) store_chunk(sbase);
+        if (!bad) split(raw0 + (uint32_t)(c % UM_RS) * raw_bytes, sbase);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         if (__syncthreads_or(bad)) break;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t dacc = tmem + (uint32_t)(a * ntmax);
             const uint32_t ahi = sbase, alo = sbase + UM_AHALF;
-            const uint32_t bhi = sbase + 2 * UM_AHALF, blo = bhi + (uint32_t)ntmax * 128u;
+            const uint32_t bhi = sbase + 2 * UM_AHALF, blo = bhi + (uint32_t)ntmax * (UM_KC * 4);
 #pragma unroll
             for (int j = 0; j < UM_KC / 8; ++j) {
                 const uint32_t k = (uint32_t)j * 2 * UM_LBO;
@@ -416,14 +461,9 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             }
             umma_commit(&bar[s]);
         }
-        ++c;
-        if (++kc == cur.nk) {
-            kc = 0;
-            if (++p == p1) break;
-            cur = pair_at(p);
-        }
-        load_chunk(cur, kc);  // in flight while the products of chunk c - 1 run
+        issue();  // chunk c + UM_RS - 1 into the raw stage chunk c - 1 used
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     // the last commit completes after every product issued before it
     if (!bad && c > 0) bad = !mbar_wait(&bar[(c - 1) & 1], ((c - 1) >> 1) & 1);
     bad = __syncthreads_or(bad);
@@ -489,7 +529,10 @@ cudaError_t launch_i2o_umma(bool cplx, const DMap &m, const DSide &recv, const D
     const int ntiles = (W * nq + UM_NT_MAX - 1) / UM_NT_MAX;
     const int qt_max = (nq + ntiles - 1) / ntiles;
     const int ntmax = ((W * qt_max + 15) / 16) * 16;
-    const size_t smem = 2 * (2 * (size_t)UM_AHALF + 2 * (size_t)ntmax * 128);
+    const int lbmax = cplx ? ((qt_max + 7) / 8) * 8 : ntmax;
+    // two split buffers (A and B, TF32 hi and lo) and UM_RS raw stages
+    const size_t smem = 2 * (2 * (size_t)UM_AHALF + 2 * (size_t)ntmax * (UM_KC * 4)) +
+                        (size_t)UM_RS * (UM_RAWA + (size_t)lbmax * UM_RAWROW);
     const dim3 grid(nnodes, (maxcoef + UM_M - 1) / UM_M, ntiles);
     auto go = [&](auto kern, auto *am, auto *dm) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
