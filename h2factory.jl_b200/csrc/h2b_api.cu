@@ -143,7 +143,7 @@ struct h2b_workspace {
     void *xnear = nullptr;  // gathered x rows for the tensor-core near kernel (real, >= 8 RHS)
     std::atomic<int> busy{0};
     cudaStream_t aux = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr, ev_far = nullptr;
     std::vector<void *> allocs;
 };
 
@@ -1090,6 +1090,7 @@ h2b_status h2b_workspace_destroy(h2b_workspace *ws) {
     if (ws->aux) cudaStreamDestroy(ws->aux);
     if (ws->ev_fork) cudaEventDestroy(ws->ev_fork);
     if (ws->ev_join) cudaEventDestroy(ws->ev_join);
+    if (ws->ev_far) cudaEventDestroy(ws->ev_far);
     if (ws->ev_done) cudaEventDestroy(ws->ev_done);
     delete ws;
     (void)cudaGetLastError();  // teardown reports nothing to later calls
@@ -1126,9 +1127,15 @@ h2b_status h2b_workspace_create(h2b_core *core, int32_t max_nrhs, h2b_workspace 
     if (e == cudaSuccess) e = al(&ws->ybuf, ndof * vsz);
     if (e == cudaSuccess && !cplx && max_nrhs >= 8)
         e = al(&ws->xnear, (size_t)std::max(core->test.ndofs, core->trial.ndofs) * 16 * sizeof(double));
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ws->aux, cudaStreamNonBlocking);
+    // the far passes (a chain of dependent launches, the critical path) run on this stream at the
+    // device's greatest priority, so their blocks are scheduled ahead of the near field's, which
+    // fills the SMs around them
+    int prio_least = 0, prio_greatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ws->aux, cudaStreamNonBlocking, prio_greatest);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_far, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_done, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         h2b_workspace_destroy(ws);
@@ -1253,12 +1260,16 @@ h2b_status run(h2b_workspace *ws, Kind kind, int32_t mode, int32_t nrhs, const v
             s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(aA, a), b, st, nullptr);
         }
     } else {
-        // near on the auxiliary stream, far on the caller's; the leaf scatter waits for the near
+        // near on the caller's stream, far on the high-priority auxiliary stream; the far leaf
+        // scatter waits for the near product, and the caller's stream for the far passes
         CUDA_TRY(cudaEventRecord(ws->ev_fork, st));
         CUDA_TRY(cudaStreamWaitEvent(ws->aux, ws->ev_fork, 0));
-        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b, ws->xnear, ws->aux));
-        CUDA_TRY(cudaEventRecord(ws->ev_join, ws->aux));
-        s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(aA, a), cdouble{1.0, 0.0}, st, ws->ev_join);
+        CUDA_TRY(launch_near(cplx, mode, c->dnear, rows.d, cols.d, nrhs, x, ldx, y, ldy, a, b, ws->xnear, st));
+        CUDA_TRY(cudaEventRecord(ws->ev_join, st));
+        s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(aA, a), cdouble{1.0, 0.0}, ws->aux, ws->ev_join);
+        if (s) return s;
+        CUDA_TRY(cudaEventRecord(ws->ev_far, ws->aux));
+        CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_far, 0));
     }
     if (s) return s;
     if (cap == cudaStreamCaptureStatusNone) CUDA_TRY(cudaEventRecord(ws->ev_done, st));
