@@ -48,6 +48,7 @@ constexpr uint32_t UM_AHALF = UM_M * UM_KC * 4;  // bytes of one A split part (8
 constexpr uint32_t UM_RAWROW = UM_KC * 4 + 16;   // raw row layout: 64 bytes + 16 of padding
 constexpr uint32_t UM_RAWA = UM_M * UM_RAWROW;   // raw A bytes (>= the column layouts' 8,448)
 constexpr unsigned UM_SPIN = 1u << 22;           // try_wait attempts before a wait gives up
+constexpr int UM_XMAP = 512;     // moment-row permutations up to this length are read from shared memory
 
 __device__ unsigned int g_umma_timeouts = 0;
 
@@ -200,6 +201,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     __shared__ uint64_t bar[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int nchunks_s;
+    __shared__ int xmap_s[UM_XMAP];  // the copied pair's moment-row permutation
 
     const int node = nodes[blockIdx.x];
     const int nc = um_ncoef(r, r.level[node]);
@@ -281,22 +283,35 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     const int arow_f = tid & (UM_M - 1);                       // forward: the thread's row
     const int arow_t0 = (warp & 7) * 8 + (lane & 7);           // transposed: rows arow_t0, + 64
     const uint32_t colstride = UM_M * EB + 16;                 // raw column layout: bytes per k
-    int pp = p0, pk = 0, issued = 0;  // copy cursor: pair, chunk within it, chunks issued
-    UmPair<T> pu = pair_at(p0);
-    int hrow[2];
-    auto load_rows = [&]() {
+    // copy cursor: pair pp, its chunk pk, chunks issued; the next pair's operands and row map are
+    // fetched a pair ahead (their loads complete while the current pair streams), and a permuted
+    // pair's moment-row map is staged in shared memory once per pair
+    int pp = p0, pk = 0, issued = 0;
+    UmPair<T> pu = pair_at(p0), pn = pu;
+    int hrow[2], hrow_n[2];
+    auto rows_of = [&](const UmPair<T> &u, int (&h)[2]) {
         if (fwd) {
-            hrow[0] = arow_f < mt ? (pu.rowmap ? pu.rowmap[m0 + arow_f] : m0 + arow_f) : 0;
-            hrow[1] = 0;
+            h[0] = arow_f < mt ? (u.rowmap ? u.rowmap[m0 + arow_f] : m0 + arow_f) : 0;
+            h[1] = 0;
         } else {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int rr = arow_t0 + 64 * h;
-                hrow[h] = rr < mt ? (pu.rowmap ? pu.rowmap[m0 + rr] : m0 + rr) : 0;
+            for (int e = 0; e < 2; ++e) {
+                const int rr = arow_t0 + 64 * e;
+                h[e] = rr < mt ? (u.rowmap ? u.rowmap[m0 + rr] : m0 + rr) : 0;
             }
         }
     };
-    load_rows();
+    auto fill_xmap = [&]() {  // every thread calls it (one barrier)
+        if (pu.xmap && pu.snc <= UM_XMAP)
+            for (int k = tid; k < pu.snc; k += UM_THREADS) xmap_s[k] = pu.xmap[k];
+        __syncthreads();
+    };
+    rows_of(pu, hrow);
+    if (p0 + 1 < p1) {
+        pn = pair_at(p0 + 1);
+        rows_of(pn, hrow_n);
+    }
+    fill_xmap();
     const uint32_t smem0 = su32(um_smem);
     const uint32_t raw0 = smem0 + 2 * split_bytes;
     auto issue = [&]() {  // copies of the next chunk into raw stage (issued % UM_RS); one group
@@ -326,15 +341,24 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
                 const int q = (w % nrb) * 8 + (l & 7), kq = (w / nrb) * 4 + (l >> 3), k = kq0 + kq;
                 const bool ok = q < qt && k < pu.snc;
                 const T *src = pu.X;
-                if (ok) src = pu.X + (int64_t)q * pu.snc + (pu.xmap ? pu.xmap[k] : k);
+                if (ok)
+                    src = pu.X + (int64_t)q * pu.snc +
+                          (pu.xmap ? (pu.snc <= UM_XMAP ? xmap_s[k] : pu.xmap[k]) : k);
                 cp_elem<EB>(rb + (uint32_t)q * UM_RAWROW + (uint32_t)kq * EB, src, ok);
             }
             ++issued;
             if (++pk == pu.nk) {
                 pk = 0;
                 if (++pp < p1) {
-                    pu = pair_at(pp);
-                    load_rows();
+                    pu = pn;
+                    hrow[0] = hrow_n[0];
+                    hrow[1] = hrow_n[1];
+                    if (pp + 1 < p1) {
+                        pn = pair_at(pp + 1);
+                        rows_of(pn, hrow_n);
+                    }
+                    __syncthreads();  // every thread's copies read the previous pair's map
+                    fill_xmap();
                 }
             }
         }
