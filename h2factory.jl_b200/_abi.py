@@ -76,7 +76,7 @@ EXPORTS = [
     "h2b_version", "h2b_last_error", "h2b_core_create", "h2b_core_destroy", "h2b_core_get_info",
     "h2b_workspace_create", "h2b_workspace_destroy", "h2b_matvec", "h2b_matvec_host",
     "h2b_farmul", "h2b_nearmul", "h2b_farmul_noalloc", "h2b_map_blob_write", "h2b_map_blob_read",
-    "h2b_core_create_from_blob", "h2b_tensor_wait_timeouts",
+    "h2b_core_create_from_blob", "h2b_tensor_wait_timeouts", "h2b_matvec_host_async",
 ]
 
 H2B_NOALLOC_SCRATCH_BYTES = 16 << 20
@@ -122,7 +122,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.h2b_workspace_destroy.argtypes = [vp]
     lib.h2b_tensor_wait_timeouts.argtypes = [C.c_int32, C.POINTER(C.c_uint32)]
     mv = [vp, C.c_int32, C.c_int32, vp, C.c_int64, vp, C.c_int64, _f64p, _f64p, vp]
-    for name in ("h2b_matvec", "h2b_matvec_host", "h2b_farmul", "h2b_nearmul"):
+    for name in ("h2b_matvec", "h2b_matvec_host", "h2b_matvec_host_async", "h2b_farmul", "h2b_nearmul"):
         getattr(lib, name).argtypes = mv
     # far part in the library's built-in scratch: takes the core instead of a workspace
     lib.h2b_farmul_noalloc.argtypes = mv

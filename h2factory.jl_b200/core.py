@@ -484,6 +484,24 @@ class H2Workspace:
                                             nin, y.ctypes.data_as(C.c_void_p), nout, a, b, None))
         return y
 
+    def matvec_host_async(self, x: np.ndarray, y: np.ndarray, mode: int = _abi.H2B_FORWARD, stream=None,
+                          alpha=None, beta=None) -> None:
+        """Enqueue mul! on host arrays on `stream` (h2b_matvec_host_async) and return at once.
+
+        x and y are Fortran-ordered arrays (page-locked memory for asynchronous copies) that must
+        stay alive and untouched until the stream has passed this work."""
+        nrow, ncol = self.shape
+        nout, nin = (nrow, ncol) if mode == _abi.H2B_FORWARD else (ncol, nrow)
+        if not (x.flags.f_contiguous and y.flags.f_contiguous) or x.dtype != self.core.dtype or y.dtype != x.dtype:
+            raise ValueError("x and y must be Fortran-ordered arrays of the map's dtype")
+        nrhs = 1 if x.ndim == 1 else x.shape[1]
+        if x.shape[0] != nin or y.shape[0] != nout or (1 if y.ndim == 1 else y.shape[1]) != nrhs:
+            raise ValueError("x / y shapes do not match the map")
+        a, b = _alphabeta(alpha, beta)
+        _abi.check(self.lib.h2b_matvec_host_async(self.handle, mode, nrhs, x.ctypes.data_as(C.c_void_p),
+                                                  nin, y.ctypes.data_as(C.c_void_p), nout, a, b,
+                                                  C.c_void_p(stream)))
+
 
 class OrientedMap:
     """transpose(A) or adjoint(A) of a workspace (LinearMaps' TransposeMap / AdjointMap)."""

@@ -1295,9 +1295,13 @@ h2b_status h2b_nearmul(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void
     return run(ws, KIND_NEAR, mode, nrhs, x, ldx, y, ldy, alpha, beta, stream);
 }
 
-h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
-                           int64_t ldx, void *y, int64_t ldy, const double *alpha,
-                           const double *beta, void *stream) {
+// Host arrays in and out: copy x into the workspace's staging buffer, multiply, copy y out, all
+// on `stream`; `wait` synchronises the stream before returning (h2b_matvec_host), otherwise the
+// workspace's completion event is moved past the copy out so the next call on this workspace
+// cannot overwrite the staging buffers early (h2b_matvec_host_async).
+static h2b_status matvec_host_impl(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
+                                   int64_t ldx, void *y, int64_t ldy, const double *alpha,
+                                   const double *beta, void *stream, bool wait) {
     if (!ws || !x || !y) return fail(H2B_ERR_INVALID, "null argument");
     if (mode < 0 || mode > 2) return fail(H2B_ERR_INVALID, "mode must be 0, 1 or 2");
     if (nrhs < 1 || nrhs > ws->max_nrhs)
@@ -1320,8 +1324,26 @@ h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const 
                        /*take_busy=*/false);
     if (s) return s;
     CUDA_TRY(cudaMemcpy2DAsync(y, ldy * vsz, ws->ybuf, nout * vsz, nout * vsz, nrhs, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    if (wait) {
+        CUDA_TRY(cudaStreamSynchronize(st));
+    } else {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+        if (cap == cudaStreamCaptureStatusNone) CUDA_TRY(cudaEventRecord(ws->ev_done, st));
+    }
     return H2B_OK;
+}
+
+h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
+                           int64_t ldx, void *y, int64_t ldy, const double *alpha,
+                           const double *beta, void *stream) {
+    return matvec_host_impl(ws, mode, nrhs, x, ldx, y, ldy, alpha, beta, stream, true);
+}
+
+h2b_status h2b_matvec_host_async(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
+                                 int64_t ldx, void *y, int64_t ldy, const double *alpha,
+                                 const double *beta, void *stream) {
+    return matvec_host_impl(ws, mode, nrhs, x, ldx, y, ldy, alpha, beta, stream, false);
 }
 
 }  // extern "C"

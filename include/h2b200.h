@@ -265,6 +265,17 @@ h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const 
                            int64_t ldx, void *y, int64_t ldy, const double *alpha,
                            const double *beta, void *stream);
 
+/* h2b_matvec_host without the final wait: enqueues on `stream` the copy of x into the workspace,
+ * the product and the copy of the result into y, and returns. x and y must stay valid and
+ * untouched until the stream has passed this work (synchronize the stream or an event recorded on
+ * it); with pinned (page-locked) host memory the copies are asynchronous, so a serving loop that
+ * gives each of two workspaces its own stream overlaps one request's copies with another's
+ * product. A later call on the same workspace, on any stream, waits for this one's copy out.
+ * No counterpart in the reference, whose mul! returns when y is written. */
+h2b_status h2b_matvec_host_async(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
+                                 int64_t ldx, void *y, int64_t ldy, const double *alpha,
+                                 const double *beta, void *stream);
+
 /* Far part only: farmul! (src/farinteractions/farmul.jl:8-70). With alpha = beta = NULL y is
  * zero-filled first (3-argument form); otherwise only leaves that receive a far contribution
  * are updated, y_leaf = α α(A) far + β y_leaf. */
