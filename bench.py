@@ -308,7 +308,8 @@ def served_run(torch, h2, core, nrhs, steps, warmup, device, seed, inflight):
     `inflight` of them on the device at once (request i on workspace and stream i % inflight, as a
     serving loop runs them). Device events: per-request latency on its stream, and the total from
     one start event that every stream waits for to the last request's end."""
-    wss = [h2.H2Workspace(core, max_nrhs=nrhs, device=int(device.split(":")[1])) for _ in range(inflight)]
+    dcore = h2.DeviceCore(core, int(device.split(":")[1]))  # one resident core, one workspace per request slot
+    wss = [h2.H2Workspace(dcore, max_nrhs=nrhs) for _ in range(inflight)]
     n = core.trial.npoints
     rng = np.random.default_rng(seed)
     xh = rng.standard_normal((n, nrhs))
@@ -447,6 +448,20 @@ def gpu_arm(args, rank, world, local_rank):
 
     serving = serving_leg(torch, h2, core32, local_rank, args) if args.serve_seconds > 0 else None
 
+    # the serving autotuner's choice for this map (block width, requests in flight), timed on the
+    # resident core; informational: the timed forms above use --nrhs and --inflight
+    tuned = None
+    if args.autotune:
+        from h2factory_b200 import autotune
+
+        tuner = autotune.Autotuner(measure=lambda c, b, f: autotune.measure_on_device(
+            c, b, f, steps=12, warmup=2, device=local_rank, dcore=wsl[0].dcore))
+        ch = tuner.choose(core32, nserve, blocks=(1, 4, 8, 16), inflight=(1, 2, 3))
+        tuned = {"key": ch["key"], "block": ch["block"], "inflight": ch["inflight"],
+                 "rhs_per_s": ch["rhs_per_s"], "p99_ms": ch["p99_ms"],
+                 "trials": [(t["block"], t["inflight"], round(t["rhs_per_s"]), round(t["p99_ms"], 3))
+                            for t in ch["trials"]]}
+
     # the same map with a matrix-free near field (entries recomputed from the points, no stored
     # blocks): its own form, reported beside the stored-block forms
     mf = None
@@ -510,6 +525,8 @@ def gpu_arm(args, rank, world, local_rank):
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if serving is not None:
         line["serving"] = serving
+    if tuned is not None:
+        line["autotune"] = tuned
     print(json.dumps(line), flush=True)
 
 
@@ -641,6 +658,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nrhs", type=int, default=16, help="right-hand sides per served block")
     ap.add_argument("--inflight", type=int, default=2, help="served requests on the device at once")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip the autotuner's report of block width and requests in flight")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-check", action="store_true")
     ap.add_argument("--n", type=int, default=262144, help="points (smaller cases are for profiling)")

@@ -8,6 +8,7 @@ The package directory is `h2factory.jl_b200/`; it is imported as `h2factory_b200
 * `core`     -- H2Core (read-only map data), DeviceCore, H2Workspace, mul_/farmul_/nearmul_,
                 transpose/adjoint views: H2Factory's map API over the C ABI;
 * `_abi`     -- ctypes mirror of include/h2b200.h and the library loader;
+* `autotune` -- per-shape choice of the serving block width and requests in flight, cached;
 * `build`    -- compiles csrc/ into libh2b200.so (sm_100a).
 """
 
@@ -16,5 +17,6 @@ from .core import (H2Core, DeviceCore, H2Workspace, OrientedMap, adjoint, farmul
                    map_blob, mul_, nearmul_, read_blob, save_map, similarworkspace, transpose)
 from . import methods  # noqa: F401
 from . import batch  # noqa: F401
+from . import autotune  # noqa: F401
 from ._abi import (H2B_ADJOINT as ADJOINT, H2B_FORWARD as FORWARD,  # noqa: F401
                    H2B_TRANSPOSE as TRANSPOSE, H2BError, WorkspaceBusyError)
