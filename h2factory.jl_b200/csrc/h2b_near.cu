@@ -219,8 +219,11 @@ __global__ void near_gather_kernel(const int *__restrict__ value, int nvals, int
 // Fragment row g of row tile t is slab row 4g + t, so a lane reads its 4 rows with two 16-byte
 // loads. Rows and columns past the block are zero-filled by the copies (source size 0). Waits are
 // on the warp's own copies (cp.async.wait_group, then __syncwarp). On the benchmark map this form
-// is 4 % faster per served step than the same tiling with register-staged loads.
-constexpr int MST = 3;                 // stages per warp
+// is 4 % faster per served step than the same tiling with register-staged loads. Two stages per
+// warp keep the CTA at 59 KB of shared memory and 78 registers, so three CTAs (24 warps) share an
+// SM: 11 % faster for 16 right-hand sides than three stages at two CTAs per SM (837 vs 941 us on
+// the benchmark map); four CTAs of 4-column stages spill and measured slower.
+constexpr int MST = 2;                 // stages per warp
 constexpr int MCOLS = 8;               // columns per stage
 constexpr int MSA = 34;                // slab column stride (doubles): 16-byte fragment reads hit
                                        // the banks 4 lanes each, the minimum for 512 bytes
@@ -238,7 +241,7 @@ constexpr size_t mma_pipe_smem() {  // all warps' rings (also holds the partial 
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NEAR_WARPS * 32, 2)
+__global__ void __launch_bounds__(NEAR_WARPS * 32, 3)
 near_rows_mma_kernel(NearOp op, DSide outs, DSide ins, int r0, int rc, const double *__restrict__ xp,
                           double *__restrict__ y, int64_t ldy, double alpha, double beta, bool beta_zero) {
     constexpr int R = 8 * NT;
