@@ -609,6 +609,65 @@ def sphere_core(n, device, precision="fp64"):
     return h2, core
 
 
+def batched_arm(args):
+    """The batched-uneven configuration's shape: `--maps` maps drawn as that configuration draws them
+    (point counts log-uniform in [2048, --nmax], unit-cube volume / sphere surface / 4:1:1 ellipsoid
+    surface, Laplace or Helmholtz with k uniform in [1, 20], Chebyshev p in {4, 5, 6}, leaves of at
+    most 64 points, 1-16 right-hand sides, orientations mixed), FP32 far field, near blocks
+    assembled on the device. A pass is every map's product once; it is timed as eager launches
+    (each map on its own stream) and as one replay of the batch captured in a CUDA graph."""
+    import torch
+
+    h2 = _package()
+    from h2factory_b200 import assembly, batch, methods, trees
+
+    device = "cuda:0"
+    rng = np.random.default_rng(2026)
+    cores, nrhs, modes, shapes = [], [], [], []
+    for _ in range(args.maps):
+        n = int(np.exp(rng.uniform(np.log(2048), np.log(args.nmax))))
+        geometry = ("cube", "sphere", "ellipsoid")[rng.integers(3)]
+        if geometry == "cube":
+            pts = rng.random((n, 3))
+        else:
+            i = np.arange(n) + 0.5
+            phi, th = np.arccos(1 - 2 * i / n), np.pi * (1 + 5 ** 0.5) * i
+            sp = np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], axis=1)
+            sp = sp + 0.1 * np.sqrt(4 * np.pi / n) * rng.standard_normal(sp.shape)
+            pts = 0.5 + sp * (np.array([0.45, 0.45, 0.45]) if geometry == "sphere" else np.array([0.45, 0.1125, 0.1125]))
+        helm = rng.random() >= 0.5
+        k = float(rng.uniform(1, 20)) if helm else 0.0
+        p = int(rng.integers(4, 7))
+        tree = trees.build_tree(pts, maxvalues=64, root_center=[0.5] * 3, root_halfsize=0.5)
+        core = methods.interpolation_core(tree, methods.helmholtz(k) if helm else methods.laplace, p, near="none",
+                                          symmetry=True, precision="fp32")
+        assembly.near_blocks_device(core, "helmholtz" if helm else "laplace", wavenumber=k, device=device)
+        cores.append(core)
+        nrhs.append(int(rng.integers(1, 17)))
+        modes.append(int(rng.integers(3)))
+        shapes.append(n)
+    b = batch.BatchedMaps(cores, nrhs, device=0, modes=modes)
+    b.set_inputs([torch.randn(x.shape[1], x.shape[0], dtype=x.dtype, device=device).t() for x in b.inputs])
+    stream = torch.cuda.current_stream(device)
+    per_e, tot_e = time_loop(torch, lambda i: b.run_eager(), args.steps, args.warmup, stream)
+    b.capture()
+    per_g, tot_g = time_loop(torch, lambda i: b.replay(), args.steps, args.warmup, stream)
+    rhs = b.rhs_total()
+    print(json.dumps({
+        "metric": METRIC, "value": rhs * args.steps / (tot_g * 1e-3), "unit": "RHS/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_g / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 far / f64 near", "data": "synthetic (seeded)",
+        "config": {"workload": f"batched-uneven-{args.maps}maps-N2048-{args.nmax}", "maps": args.maps,
+                   "points_total": int(sum(shapes)), "rhs_per_pass": rhs,
+                   "step": "one pass: every map's product once",
+                   "scale": "point counts up to --nmax (the configuration draws up to 262,144)"},
+        "graph": {"rhs_per_s": rhs * args.steps / (tot_g * 1e-3), "ms_per_pass": tot_g / args.steps,
+                  "p50_ms": pct(per_g, 50), "p99_ms": pct(per_g, 99)},
+        "eager": {"rhs_per_s": rhs * args.steps / (tot_e * 1e-3), "ms_per_pass": tot_e / args.steps,
+                  "p50_ms": pct(per_e, 50), "p99_ms": pct(per_e, 99)}}), flush=True)
+    b.close()
+
+
 def sphere_arm(args):
     """Dense (Chebyshev) far field on the sphere configuration's shape: FP64 and FP32 forms, 32
     complex right-hand sides per matvec, forward/adjoint alternating (device timing)."""
@@ -668,6 +727,10 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving leg length (0: skip)")
     ap.add_argument("--no-matrix-free", dest="matrix_free", action="store_false",
                     help="skip the matrix-free near-field forms")
+    ap.add_argument("--batched", action="store_true",
+                    help="time the batched-uneven configuration's shape (eager vs one graph replay per pass)")
+    ap.add_argument("--maps", type=int, default=96, help="maps of the batched mode")
+    ap.add_argument("--nmax", type=int, default=16384, help="largest point count of the batched mode")
     ap.add_argument("--sphere", action="store_true",
                     help="time the sphere configuration's shape at --n points instead (dense far field)")
     args = ap.parse_args()
@@ -680,6 +743,9 @@ def main():
         return
     if args.sphere:
         sphere_arm(args)
+        return
+    if args.batched:
+        batched_arm(args)
         return
     if world > 1:
         import datetime

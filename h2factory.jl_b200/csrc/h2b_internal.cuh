@@ -176,7 +176,7 @@ cudaError_t launch_toeplitz_out(bool cplx, int precision, const DMap &m, const D
                                 const int *nodes, int nnodes, bool inverse, const FarArgs &fa,
                                 int maxtsize, int maxaxis, cudaStream_t st);
 // Dense I2O of the FP32 form on the tcgen05 tensor cores (h2b_umma.cu): taken when the coupling
-// storage is dense and the right-hand sides fill an MMA of N >= 16 FP32 columns.
+// storage is dense and the right-hand sides make at least 4 FP32 columns (MMA N padded to 16).
 bool i2o_umma_eligible(bool cplx, int precision, const DMap &m, int nq);
 cudaError_t launch_i2o_umma(bool cplx, const DMap &m, const DSide &recv, const DSide &src, const int *nodes,
                             int nnodes, const FarArgs &fa, int maxcoef, cudaStream_t st);

@@ -541,7 +541,10 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
 }
 
 bool i2o_umma_eligible(bool cplx, int precision, const DMap &m, int nq) {
-    return precision == H2B_FP32 && m.coupling_kind == H2B_COUPLING_DENSE && (cplx ? 2 : 1) * nq >= 16;
+    // from 4 FP32 columns (2 complex right-hand sides) the MMA tile (padded to N = 16) beats the
+    // FP64 mma.sync tile path (sphere shape at 32,768 points, 2-4 complex RHS: 16.2 vs 20.5 ms per
+    // product); a single right-hand side stays on the FMA tile path (11.9 vs 14.7 ms)
+    return precision == H2B_FP32 && m.coupling_kind == H2B_COUPLING_DENSE && (cplx ? 2 : 1) * nq >= 4;
 }
 
 cudaError_t launch_i2o_umma(bool cplx, const DMap &m, const DSide &recv, const DSide &src, const int *nodes,

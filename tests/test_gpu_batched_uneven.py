@@ -7,7 +7,7 @@ points, 1-16 right-hand sides, FP64 (plain) and FP32 (chosen) far fields, forwar
 adjoint orientations mixed. The whole batch is captured once as a CUDA graph and replayed; each
 map's replayed product must equal its eager product bit for bit, the FP64 maps the oracle
 (relative L2 1e-12), and the FP32 maps their FP64 twins within 1e-6 (their far fields run on
-the tcgen05 kernel when the right-hand sides fill 16 FP32 columns)."""
+the tcgen05 kernel when the right-hand sides make at least 4 FP32 columns)."""
 
 import copy
 

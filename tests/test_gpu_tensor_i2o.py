@@ -1,7 +1,8 @@
 """Dense I2O of the FP32 form on the tcgen05 tensor cores (three-term TF32 split), GPU.
 
 The FP32 form takes the tensor-core kernel when its couplings are dense and the right-hand sides
-fill an MMA of at least 16 FP32 columns (real maps: >= 16 right-hand sides, complex: >= 8). Each
+make at least 4 FP32 columns (real maps: >= 4 right-hand sides, complex: >= 2; the MMA's N is
+padded to 16). Each
 case multiplies in every orientation and is compared with the FP64 form of the same map, which
 test_gpu_parity.py pins to the oracle at 1e-12, and the sphere case directly with the oracle.
 Tolerances: the whole product within 1e-6 relative L2 of the FP64 result (the served form's bar);
@@ -45,8 +46,12 @@ def _core(cores, name):
 
 
 @pytest.mark.parametrize("name,nrhs", [
+    ("cheb-laplace-dense", 4),
+    ("cheb-laplace-dense", 7),
     ("cheb-laplace-dense", 16),
     ("cheb-laplace-dense", 130),
+    ("cheb-helmholtz", 2),
+    ("cheb-helmholtz", 3),
     ("cheb-helmholtz", 8),
     ("cheb-helmholtz", 32),
     ("cheb-helmholtz", 70),
