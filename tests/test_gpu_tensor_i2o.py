@@ -100,3 +100,22 @@ def test_tensor_i2o_repeatable(cores):
     a = run(h2.farmul_, ws32, x)
     b = run(h2.farmul_, ws32, x)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name,nrhs", [
+    ("cheb-laplace-dense", 1),
+    ("cheb-laplace-dense", 3),
+    ("cheb-helmholtz", 1),
+    ("sym-cheb-laplace", 2),
+    ("sym-cheb-helmholtz", 1),
+    ("petrov-cheb-laplace", 3),
+])
+def test_small_blocks_fp32_dense(cores, name, nrhs):
+    """Below the tensor-core kernel's range (fewer than 4 FP32 columns) the dense I2O of the FP32
+    form runs the FMA / FP64 mma.sync tile products; it still matches its FP64 product within 1e-6."""
+    core = _core(cores, name)
+    ws64 = h2.H2Workspace(core, max_nrhs=nrhs)
+    ws32 = h2.H2Workspace(_fp32(core), max_nrhs=nrhs)
+    for mode, op in ORIENT:
+        x = _x(core, nrhs, 51 + mode, mode)
+        assert rel(run(h2.mul_, op(ws32), x), run(h2.mul_, op(ws64), x)) < BAR, (name, nrhs, mode)
