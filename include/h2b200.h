@@ -31,7 +31,7 @@ typedef int h2b_status;
 #define H2B_ERR_CUDA 2        /* a CUDA runtime call failed                                     */
 #define H2B_ERR_NOMEM 3       /* device allocation failed or the memory budget was exceeded     */
 #define H2B_BUSY 4            /* the workspace is in use (H2Factory's ConcurrentWorkspaceError) */
-#define H2B_ERR_UNSUPPORTED 5 /* valid request this build does not implement                   */
+#define H2B_ERR_UNSUPPORTED 5 /* valid request the library does not implement                 */
 
 /* Scalar field of x, y, leaf collections, level transfers, couplings and near blocks. */
 #define H2B_REAL 0    /* double                        */
