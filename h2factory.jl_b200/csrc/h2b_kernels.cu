@@ -175,6 +175,61 @@ __device__ __forceinline__ void mma_store(const MmaAcc<A> &acc, int mt, int nq, 
         }
 }
 
+// A 64 x 16 output tile on the FP64 tensor cores held by ONE warp, operands read straight from
+// global memory (no shared-memory staging, no block barrier): acc += op(A) B, 8 row tiles x 2
+// column tiles of mma.sync m8n8k4 per k step of 4. a(i, k) and b(k, q) return the operands; rows
+// >= M, columns >= nq and k >= K read as zero. Lane fragments as in dmma8: A[g4][t4], B[t4][g4],
+// so acc[t][u][h] is C[8t + g4][8u + 2 t4 + h]. Each k step issues its 10 loads per lane before
+// its 16 products, and the loop is unrolled twice, so loads of the next step overlap the products.
+// For the small real products of the transfers and leaves with 2-16 right-hand sides, where a
+// CTA-wide staged tile waits on one load round trip per 32-wide chunk.
+template <class ALoad, class BLoad>
+__device__ __forceinline__ void warp_mma64x16(int M, int K, int nq, ALoad a, BLoad b, double (&acc)[8][2][2]) {
+    const int lane = threadIdx.x & 31, g4 = lane >> 2, t4 = lane & 3;
+#pragma unroll 2
+    for (int k0 = 0; k0 < K; k0 += 4) {
+        const int k = k0 + t4;
+        const bool kin = k < K;
+        double af[8], bf[2];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int i = 8 * t + g4;
+            af[t] = kin && i < M ? a(i, k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int q = 8 * u + g4;
+            bf[u] = kin && q < nq ? b(k, q) : 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) dmma8(acc[t][u], af[t], bf[u]);
+    }
+}
+
+__device__ __forceinline__ void warp_acc_zero(double (&acc)[8][2][2]) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
+}
+
+// f(i, q, value) for every element of the warp's tile inside M x nq
+template <class F>
+__device__ __forceinline__ void warp_acc_store(const double (&acc)[8][2][2], int M, int nq, F f) {
+    const int lane = threadIdx.x & 31, g4 = lane >> 2, t4 = lane & 3;
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = 8 * t + g4, q = 8 * u + 2 * t4 + h;
+                if (i < M && q < nq) f(i, q, acc[t][u][h]);
+            }
+}
+
 // op(M)[i, k] = M[i + k*ldm] (trans = false) or M[k + i*ldm] (trans = true), conjugated when cjg.
 template <class T, class A, class XLoad>
 __device__ __forceinline__ void tile_gemm(const T *__restrict__ M, int64_t ldm, bool trans, bool cjg, int m0,
@@ -397,6 +452,145 @@ __global__ void transfer_up_kernel(DMap m, DSide s, const int *__restrict__ node
         for (int e = threadIdx.x; e < nout; e += blockDim.x) narrow(acc[e], mp[(int64_t)q * nout + e]);
         __syncthreads();
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Real maps, dense transfers and leaf collections of at most 64 coefficients, 2-16 right-hand
+// sides: the same products one warp per child / leaf (warp_mma64x16). A2 sums a parent's children
+// in a fixed order (warp w holds child w) through shared memory; C1 and A1 write their tiles from
+// registers.
+// ---------------------------------------------------------------------------------------------
+constexpr int WARP_TILE = 64 * 16;  // doubles of one warp's 64 x 16 tile
+
+template <class T>
+__global__ void __launch_bounds__(256)
+transfer_up_warp_kernel(DMap m, DSide s, const int *__restrict__ nodes, int nrhs, T *__restrict__ am) {
+    extern __shared__ double wpart[];  // [8 warps][q * 64 + i]
+    const int p = nodes[blockIdx.x];
+    const int lp = s.level[p], lc = lp + 1;
+    const int nout = ncoef_of(s, lp), nin = ncoef_of(s, lc);
+    const int nq = m.ncomp * nrhs;
+    const int c0 = s.child_ptr[p], c1 = s.child_ptr[p + 1];
+    const int warp = threadIdx.x >> 5;
+    double acc[8][2][2];
+    warp_acc_zero(acc);
+    if (c0 + warp < c1) {  // warp-uniform
+        const int ch = s.child[c0 + warp];
+        const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
+        const T *mc = am + s.mom_off[ch] * nrhs;
+        warp_mma64x16(nout, nin, nq, [&](int i, int k) -> double { return (double)Tk[i + (int64_t)k * nout]; },
+                      [&](int k, int q) -> double { return (double)mc[(int64_t)q * nin + k]; }, acc);
+    }
+    double *pw = wpart + warp * WARP_TILE;
+    warp_acc_store(acc, 64, 16, [&](int i, int q, double v) { pw[q * 64 + i] = v; });
+    __syncthreads();
+    T *mp = am + s.mom_off[p] * nrhs;
+    for (int e = threadIdx.x; e < nout * nq; e += blockDim.x) {
+        const int i = e % nout, q = e / nout;
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) v += wpart[w * WARP_TILE + q * 64 + i];
+        narrow(v, mp[(int64_t)q * nout + i]);
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256)
+transfer_down_warp_kernel(DMap m, DSide s, const int *__restrict__ nodes, int nnodes,
+                          const uint8_t *__restrict__ received, int nrhs, T *__restrict__ dm) {
+    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (idx >= nnodes) return;  // whole warp; no block barrier
+    const int c = nodes[idx];
+    const int lc = s.level[c], lp = lc - 1;
+    const int par = s.parent[c];
+    const int nout = ncoef_of(s, lc), nin = ncoef_of(s, lp);
+    const bool acc0 = received[c] != 0;
+    const T *Tk = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[c]];
+    T *mc = dm + s.mom_off[c] * nrhs;
+    const T *mp = dm + s.mom_off[par] * nrhs;
+    const int nq = m.ncomp * nrhs;
+    double acc[8][2][2];
+    warp_acc_zero(acc);
+    // stored T is nin x nout (parent x child): op(T)[i, k] = T[k + i * nin]
+    warp_mma64x16(nout, nin, nq, [&](int i, int k) -> double { return (double)Tk[k + (int64_t)i * nin]; },
+                  [&](int k, int q) -> double { return (double)mp[(int64_t)q * nin + k]; }, acc);
+    warp_acc_store(acc, nout, nq, [&](int i, int q, double v) {
+        T *dst = &mc[(int64_t)q * nout + i];
+        narrow(acc0 ? (double)*dst + v : v, *dst);
+    });
+}
+
+template <class T>
+__global__ void __launch_bounds__(256)
+leaf_aggregate_warp_kernel(DMap m, DSide s, const int *__restrict__ leaves, int nleaves, int nrhs,
+                           const double *__restrict__ x, int64_t ldx, T *__restrict__ am) {
+    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (idx >= nleaves) return;  // whole warp; no block barrier
+    const int leaf = leaves[idx];
+    const int nc = ncoef_of(s, s.level[leaf]);
+    const int v0 = s.value_ptr[leaf], nv = s.value_ptr[leaf + 1] - v0;
+    const T *C = static_cast<const T *>(s.coll) + s.coll_off[leaf];
+    T *mom = am + s.mom_off[leaf] * nrhs;
+    const int *vals = s.value + v0;
+    for (int c = 0; c < m.ncomp; ++c) {
+        const T *Cc = C + (int64_t)c * nc * nv;
+        double acc[8][2][2];
+        warp_acc_zero(acc);
+        warp_mma64x16(nc, nv, nrhs, [&](int i, int k) -> double { return (double)Cc[i + (int64_t)k * nc]; },
+                      [&](int k, int q) -> double { return x[(int64_t)q * ldx + vals[k]]; }, acc);
+        warp_acc_store(acc, nc, nrhs, [&](int i, int q, double v) { narrow(v, mom[((int64_t)c * nrhs + q) * nc + i]); });
+    }
+}
+
+// C2 for leaves of any size: the warp takes the leaf's rows 64 at a time (leaves own disjoint
+// values, so no two warps write the same entry of y)
+template <class T>
+__global__ void __launch_bounds__(256)
+leaf_disaggregate_warp_kernel(DMap m, DSide s, const int *__restrict__ leaves, int nleaves, int nrhs,
+                              const T *__restrict__ dm, double alpha, double beta, bool beta_zero,
+                              double *__restrict__ y, int64_t ldy) {
+    const int idx = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (idx >= nleaves) return;  // whole warp; no block barrier
+    const int leaf = leaves[idx];
+    const int nc = ncoef_of(s, s.level[leaf]);
+    const int v0 = s.value_ptr[leaf], nv = s.value_ptr[leaf + 1] - v0;
+    const T *C = static_cast<const T *>(s.coll) + s.coll_off[leaf];
+    const T *mom = dm + s.mom_off[leaf] * nrhs;
+    const int *vals = s.value + v0;
+    for (int m0 = 0; m0 < nv; m0 += 64) {
+        const int mt = min(64, nv - m0);
+        double acc[8][2][2];
+        warp_acc_zero(acc);
+        for (int c = 0; c < m.ncomp; ++c) {
+            const T *Cc = C + (int64_t)c * nc * nv;
+            const T *mc = mom + (int64_t)c * nrhs * nc;
+            // op(C)[i, k] = C[k + i * nc]: the leaf's collection transposed
+            warp_mma64x16(mt, nc, nrhs, [&](int i, int k) -> double { return (double)Cc[k + (int64_t)(m0 + i) * nc]; },
+                          [&](int k, int q) -> double { return (double)mc[(int64_t)q * nc + k]; }, acc);
+        }
+        warp_acc_store(acc, mt, nrhs, [&](int i, int q, double v) {
+            double *dst = &y[(int64_t)q * ldy + vals[m0 + i]];
+            const double w = alpha * v;
+            *dst = beta_zero ? w : w + beta * *dst;
+        });
+    }
+}
+
+// Launchers of the warp kernels (real maps only: the complex instantiations are never referenced).
+template <class T>
+cudaError_t warp_transfer_up(const DMap &m, const DSide &s, const int *nodes, int nnodes, int nrhs, void *am,
+                             cudaStream_t st) {
+    const size_t wsm = 8 * WARP_TILE * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(transfer_up_warp_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+    if (e == cudaSuccess)
+        transfer_up_warp_kernel<T><<<nnodes, 256, wsm, st>>>(m, s, nodes, nrhs, static_cast<T *>(am));
+    return e;
+}
+template <class T>
+void warp_transfer_down(const DMap &m, const DSide &s, const int *nodes, int nnodes, const uint8_t *received,
+                        int nrhs, void *dm, cudaStream_t st) {
+    transfer_down_warp_kernel<T><<<(nnodes + 7) / 8, 256, 0, st>>>(m, s, nodes, nnodes, received, nrhs,
+                                                                   static_cast<T *>(dm));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1128,11 +1322,15 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 cudaError_t launch_leaf_aggregate(bool cplx, int precision, const DMap &m, const DSide &s,
                                   const int *leaves, int nleaves, int maxcoef, bool conjc,
                                   const FarArgs &fa, const void *x, int64_t ldx, cudaStream_t st) {
-    (void)maxcoef;
     if (nleaves == 0) return cudaSuccess;
     cudaError_t err = cudaSuccess;
     if (!cplx) {
         H2B_DISPATCH_REAL(precision, {
+            if (fa.nrhs >= 2 && fa.nrhs <= 16 && maxcoef <= 64) {
+                leaf_aggregate_warp_kernel<T><<<(nleaves + 7) / 8, 256, 0, st>>>(
+                    m, s, leaves, nleaves, fa.nrhs, static_cast<const double *>(x), ldx, static_cast<T *>(fa.am));
+                break;
+            }
             auto kern = fa.nrhs > 1 ? &leaf_aggregate_kernel<T, double, true> : &leaf_aggregate_kernel<T, double, false>;
             err = allow_smem(kern, tile_smem<double>());
             if (err == cudaSuccess)
@@ -1155,13 +1353,21 @@ cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DS
                                const int *nodes, int nnodes, bool conjt, const FarArgs &fa,
                                int maxcoef, int maxsep, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
+    // real maps, dense transfers of at most 64 coefficients, 2-16 right-hand sides: a warp per child
+    const int nqw = m.ncomp * fa.nrhs;
+    if (!cplx && m.transfer_kind == H2B_TRANSFER_DENSE && nqw >= 2 && nqw <= 16 && maxcoef <= 64 && m.nsectors <= 8) {
+        cudaError_t e = precision == H2B_FP64 ? warp_transfer_up<double>(m, s, nodes, nnodes, fa.nrhs, fa.am, st)
+                                              : warp_transfer_up<float>(m, s, nodes, nnodes, fa.nrhs, fa.am, st);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     const int bs = m.transfer_kind == H2B_TRANSFER_DENSE ? 256 : block_for(maxcoef);
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using A = typename ScalarTraits<T>::Acc;
         const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? tile_smem<A>()
                                                                  : 3 * (size_t)maxsep * sizeof(A);
-        auto kern = m.ncomp * fa.nrhs > 1 ? &transfer_up_kernel<T, true> : &transfer_up_kernel<T, false>;
+        const int nq = m.ncomp * fa.nrhs;
+        auto kern = nq > 1 ? &transfer_up_kernel<T, true> : &transfer_up_kernel<T, false>;
         err = allow_smem(kern, sm);
         if (err == cudaSuccess)
             kern<<<nnodes, bs, sm, st>>>(m, s, nodes, conjt, fa.nrhs, static_cast<T *>(fa.am));
@@ -1328,6 +1534,12 @@ cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const 
                                  const int *nodes, int nnodes, const uint8_t *received,
                                  const FarArgs &fa, int maxcoef, int maxsep, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
+    const int nqw = m.ncomp * fa.nrhs;
+    if (!cplx && m.transfer_kind == H2B_TRANSFER_DENSE && nqw >= 2 && nqw <= 16 && maxcoef <= 64) {
+        if (precision == H2B_FP64) warp_transfer_down<double>(m, s, nodes, nnodes, received, fa.nrhs, fa.dm, st);
+        else warp_transfer_down<float>(m, s, nodes, nnodes, received, fa.nrhs, fa.dm, st);
+        return cudaGetLastError();
+    }
     const int bs = m.transfer_kind == H2B_TRANSFER_DENSE ? 256 : block_for(maxcoef, 64, 256);
     const bool conjt = fa.mode == H2B_ADJOINT;
     cudaError_t err = cudaSuccess;
@@ -1335,7 +1547,8 @@ cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const 
         using A = typename ScalarTraits<T>::Acc;
         const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? tile_smem<A>()
                                                                  : 2 * (size_t)maxsep * sizeof(A);
-        auto kern = m.ncomp * fa.nrhs > 1 ? &transfer_down_kernel<T, true> : &transfer_down_kernel<T, false>;
+        const int nq = m.ncomp * fa.nrhs;
+        auto kern = nq > 1 ? &transfer_down_kernel<T, true> : &transfer_down_kernel<T, false>;
         err = allow_smem(kern, sm);
         if (err == cudaSuccess)
             kern<<<nnodes, bs, sm, st>>>(m, s, nodes, received, conjt, fa.nrhs,
@@ -1354,6 +1567,12 @@ cudaError_t launch_leaf_disaggregate(bool cplx, int precision, const DMap &m, co
     if (!cplx) {
         const bool bz = beta.x == 0.0;
         H2B_DISPATCH_REAL(precision, {
+            if (fa.nrhs >= 2 && fa.nrhs <= 16) {  // a warp per leaf
+                leaf_disaggregate_warp_kernel<T><<<(nleaves + 7) / 8, 256, 0, st>>>(
+                    m, s, leaves, nleaves, fa.nrhs, static_cast<const T *>(fa.dm), alpha.x, beta.x, bz,
+                    static_cast<double *>(y), ldy);
+                break;
+            }
             auto kern = fa.nrhs > 1 ? &leaf_disaggregate_kernel<T, double, true> : &leaf_disaggregate_kernel<T, double, false>;
             err = allow_smem(kern, tile_smem<double>());
             if (err == cudaSuccess)
