@@ -716,7 +716,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nrhs", type=int, default=16, help="right-hand sides per served block")
-    ap.add_argument("--inflight", type=int, default=2, help="served requests on the device at once")
+    ap.add_argument("--inflight", type=int, default=3,
+                    help="served requests on the device at once (3: the autotuner's choice for this map)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip the autotuner's report of block width and requests in flight")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
