@@ -1006,6 +1006,10 @@ h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
 
 }  // namespace
 
+// Device address of the no-alloc scratch array on the current device (defined with the array at
+// the end of this file); h2b_core_create calls it once so that the array is resident from then on.
+h2b_status noalloc_scratch(void **out);
+
 // =============================================================================================
 // C ABI
 // =============================================================================================
@@ -1046,6 +1050,13 @@ h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **
         c->conj_leaf = desc->conj_leaf_adjoint != 0;
         for (int m = 0; m < 3; ++m) c->alpha[m] = {desc->alpha[m][0], desc->alpha[m][1]};
         st = build_core(c, *desc);
+        if (st == H2B_OK) {
+            // Load this file's device module on the device now, with the rest of the core's
+            // memory: under lazy module loading the no-alloc scratch array is reserved when its
+            // module is first loaded, and that must not be the first h2b_farmul_noalloc call.
+            void *scratch = nullptr;
+            st = noalloc_scratch(&scratch);
+        }
         if (st) {
             c->release();
             delete c;
@@ -1355,8 +1366,6 @@ h2b_status h2b_matvec_host_async(h2b_workspace *ws, int32_t mode, int32_t nrhs, 
 // another allocator, or allocation is forbidden after start-up): the moment and spectrum arenas
 // that a workspace would allocate are carved out of one array compiled into this file instead.
 // =============================================================================================
-#include <mutex>
-
 namespace {
 
 // The scratch array (H2B_NOALLOC_SCRATCH_BYTES on every device that loads the library, until the
@@ -1365,28 +1374,24 @@ namespace {
 // asks the runtime for the address on each device instead (noalloc_scratch below).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[H2B_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kNoallocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void *g_noalloc_ptr[kNoallocMaxDevices] = {};
+}  // namespace
 
-// Device address of the scratch array on `device`, which must be the current device. Looked up
-// on the first call per device and cached; that first call should precede any stream capture.
-h2b_status noalloc_scratch(int device, void **out) {
-    if (device < 0 || device >= kNoallocMaxDevices)
-        return fail(H2B_ERR_UNSUPPORTED, "no-alloc scratch: device %d beyond the supported %d", device,
-                    kNoallocMaxDevices);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[device]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return fail(H2B_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
-                        cudaGetErrorString(e));
-        g_noalloc_ptr[device] = p;
-    }
-    *out = g_noalloc_ptr[device];
+// Device address of the scratch array on the current device. The first lookup on a device loads
+// this file's device module there (under lazy module loading), which is when the array's memory is
+// reserved; h2b_core_create makes that lookup, so a later call only reads the module's symbol
+// table and allocates nothing. The address is not cached across calls: after a device reset the
+// module is loaded again at a new address, and a fresh lookup always names the live one.
+h2b_status noalloc_scratch(void **out) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        return fail(e == cudaErrorMemoryAllocation ? H2B_ERR_NOMEM : H2B_ERR_CUDA,
+                    "cudaGetSymbolAddress of the no-alloc scratch failed: %s", cudaGetErrorString(e));
+    *out = p;
     return H2B_OK;
 }
+
+namespace {
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
@@ -1455,8 +1460,9 @@ extern "C" h2b_status h2b_farmul_noalloc(const h2b_core *core_in, int32_t mode, 
                     "the built-in scratch holds %u bytes (use a workspace and h2b_farmul instead)",
                     need, nrhs, (unsigned)H2B_NOALLOC_SCRATCH_BYTES);
     DeviceGuard guard(c->device);
+    (void)cudaGetLastError();  // a non-sticky error left by other code is not this call's
     void *base = nullptr;
-    h2b_status s = noalloc_scratch(c->device, &base);
+    h2b_status s = noalloc_scratch(&base);
     if (s) return s;
     unsigned char *b = static_cast<unsigned char *>(base);
     // Nothing in the scratch needs clearing: every pass overwrites a moment or spectrum slot

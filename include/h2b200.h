@@ -305,8 +305,11 @@ h2b_status h2b_nearmul(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void
  * Limits and rules:
  *   - the map's scratch for `nrhs` right-hand sides (two moment arenas, plus two spectrum arenas
  *     for Toeplitz couplings) must fit in H2B_NOALLOC_SCRATCH_BYTES, else H2B_ERR_UNSUPPORTED;
- *   - the first call on a device looks up the scratch array's device address for that device;
- *     make that first call before any stream capture;
+ *   - the scratch is reserved on a device when the library's device code is loaded there, which
+ *     h2b_core_create does (under lazy module loading that load would otherwise happen inside the
+ *     first call, and that call would then allocate); each call looks the address up again and
+ *     reserves nothing, so the calls also stay valid after a device reset and a new core;
+ *   - a failure to reserve the scratch fails h2b_core_create with H2B_ERR_NOMEM;
  *   - all calls on a device share the one array: calls whose work overlaps on the GPU (other
  *     streams, other host threads) race and corrupt each other's results. Serialise them.
  *   - it allocates nothing: no cudaMalloc, no cudaFree, no allocating library routine.

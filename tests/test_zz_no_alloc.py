@@ -4,8 +4,10 @@ Some hosts cannot call cudaMalloc when they multiply: their device memory is own
 allocator (a framework's caching pool), or their serving loop forbids allocation after start-up.
 The entry point runs the far passes in a scratch array compiled into the library instead of a
 workspace. This file checks, through the C ABI, that it gives the same result as the workspace
-path (h2b_farmul) on two calls in a row -- the second call finds the first call's data in the
-shared scratch -- and that a map too large for the scratch is refused with a clear error.
+path (h2b_farmul) and as the CPU oracle on two calls in a row -- the second call finds the first
+call's data in the shared scratch --, that the calls leave the device's free memory unchanged,
+that blocks of 13 right-hand sides and a map that fills the scratch almost to its end work, and
+that a map too large for the scratch is refused with a clear error.
 
 The file name sorts last so that a run stopping at the first failure has run every other test.
 """
@@ -19,12 +21,13 @@ import torch
 import h2factory_b200 as h2
 from h2factory_b200 import _abi, methods
 from h2factory_b200.trees import build_tree
+from oracle import oracle
 
 pytestmark = pytest.mark.gpu
 
 DEV = "cuda:0"
 TOL64 = 1e-12   # same bar as the FP64 parity tests
-TOL32 = 1e-5
+TOL32 = 1e-6   # FP32 far field against the FP64 products
 
 
 def _cols(a, dt):
@@ -57,38 +60,80 @@ def _maps():
     yield "chebyshev-helmholtz-fp32", core32, TOL32
 
 
+def _rel(g, w):
+    return np.linalg.norm(g - w) / np.linalg.norm(w)
+
+
+def _check_twice(core, tol, nrhs, seed=7):
+    """Two rounds of 3- and 5-argument calls in every orientation against h2b_farmul and the
+    oracle. Every tensor is made before the calls, and the workspace products run first (they load
+    every kernel the calls use), so the device's free memory must not move across the calls."""
+    ws = h2.H2Workspace(core, max_nrhs=nrhs)
+    dt = core.dtype
+    rng = np.random.default_rng(seed)
+    n = core.trial.npoints
+    a, b = (0.5 - 0.25j, 2.0 + 1.0j) if core.field == "complex" else (0.5, 2.0)
+    cases = []
+    for call in range(2):  # two calls in a row share (and reuse) the scratch
+        for mode, view in ((0, ws), (1, h2.transpose(ws)), (2, h2.adjoint(ws))):
+            xh = rng.standard_normal((n, nrhs))
+            y0 = rng.standard_normal((n, nrhs))
+            if core.field == "complex":
+                xh = xh + 1j * rng.standard_normal((n, nrhs))
+                y0 = y0 + 1j * rng.standard_normal((n, nrhs))
+            x = _cols(xh, dt)
+            want3, want5 = _cols(np.zeros((n, nrhs)), dt), _cols(y0, dt)
+            h2.farmul_(want3, view, x)
+            h2.farmul_(want5, view, x, a, b)
+            cases.append((call, mode, xh, y0, x, want3, want5,
+                          _cols(np.full((n, nrhs), np.nan), dt), _cols(y0, dt)))
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for call, mode, xh, y0, x, want3, want5, got3, got5 in cases:
+        st, err = _noalloc(ws.dcore, mode, x, got3)
+        assert st == 0, err
+        st, err = _noalloc(ws.dcore, mode, x, got5, a, b)
+        assert st == 0, err
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0, "a no-alloc call changed the device's free memory"
+    for call, mode, xh, y0, x, want3, want5, got3, got5 in cases:
+        g3, g5 = got3.cpu().numpy(), got5.cpu().numpy()
+        assert _rel(g3, want3.cpu().numpy()) < tol, (call, mode)
+        assert _rel(g5, want5.cpu().numpy()) < tol, (call, mode, "scaled")
+        if call == 0:
+            assert _rel(g3, oracle.farmul(core, xh, mode)) < tol, (mode, "oracle")
+            assert _rel(g5, oracle.farmul(core, xh, mode, a, b, y=y0)) < tol, (mode, "oracle scaled")
+    ws.close()
+    return ws
+
+
 @pytest.mark.parametrize("name", ["toeplitz-laplace", "chebyshev-helmholtz", "chebyshev-helmholtz-fp32"])
 def test_noalloc_matches_workspace_farmul_twice(name):
     core, tol = next((c, t) for n, c, t in _maps() if n == name)
-    ws = h2.H2Workspace(core, max_nrhs=3)
-    dt = core.dtype
-    rng = np.random.default_rng(7)
-    n = core.trial.npoints
-    for call in range(2):  # two calls in a row share (and reuse) the scratch
-        for mode, view in ((0, ws), (1, h2.transpose(ws)), (2, h2.adjoint(ws))):
-            xh = rng.standard_normal((n, 3))
-            if core.field == "complex":
-                xh = xh + 1j * rng.standard_normal((n, 3))
-            x = _cols(xh, dt)
-            want = _cols(np.zeros((n, 3)), dt)
-            h2.farmul_(want, view, x)
-            got = _cols(np.full((n, 3), np.nan), dt)
-            st, err = _noalloc(ws.dcore, mode, x, got)
-            assert st == 0, err
-            torch.cuda.synchronize()
-            w, g = want.cpu().numpy(), got.cpu().numpy()
-            assert np.linalg.norm(g - w) / np.linalg.norm(w) < tol, (name, call, mode)
-            # 5-argument form on a filled y
-            y0 = rng.standard_normal((n, 3)) + (1j * rng.standard_normal((n, 3)) if core.field == "complex" else 0)
-            want = _cols(y0, dt)
-            got = _cols(y0, dt)
-            a, b = (0.5 - 0.25j, 2.0 + 1.0j) if core.field == "complex" else (0.5, 2.0)
-            h2.farmul_(want, view, x, a, b)
-            st, err = _noalloc(ws.dcore, mode, x, got, a, b)
-            assert st == 0, err
-            torch.cuda.synchronize()
-            w, g = want.cpu().numpy(), got.cpu().numpy()
-            assert np.linalg.norm(g - w) / np.linalg.norm(w) < tol, (name, call, mode, "scaled")
+    _check_twice(core, tol, 3)
+
+
+def test_noalloc_thirteen_rhs_toeplitz():
+    """13 right-hand sides: the multi-RHS kernels (FP64 tensor-core sibling I2O, a partial 16-wide
+    block) take their arenas from the scratch too."""
+    core, tol = next((c, t) for n, c, t in _maps() if n == "toeplitz-laplace")
+    _check_twice(core, tol, 13, seed=11)
+
+
+def test_noalloc_scratch_almost_full():
+    """The largest block that fits: the four 256-byte aligned arenas end just inside the scratch."""
+    core, tol = next((c, t) for n, c, t in _maps() if n == "toeplitz-laplace")
+    info = h2.DeviceCore(core).info()
+    al = lambda v: (v + 255) // 256 * 256  # noqa: E731
+
+    def need(q):
+        return 2 * al(info.moment_elems * q * 8) + 2 * al(info.spectrum_elems * q * 16)
+
+    nrhs = 1
+    while need(nrhs + 1) <= _abi.H2B_NOALLOC_SCRATCH_BYTES:
+        nrhs += 1
+    assert need(nrhs) > _abi.H2B_NOALLOC_SCRATCH_BYTES * 0.9
+    _check_twice(core, tol, nrhs, seed=13)
 
 
 def test_noalloc_refuses_maps_beyond_the_scratch():
