@@ -14,7 +14,8 @@ The package directory is `h2factory.jl_b200/`; it is imported as `h2factory_b200
 
 from . import trees, _abi  # noqa: F401
 from .core import (H2Core, DeviceCore, H2Workspace, OrientedMap, adjoint, farmul_, flatten,  # noqa: F401
-                   map_blob, mul_, nearmul_, read_blob, save_map, similarworkspace, transpose)
+                   map_blob, mul_, nearmul_, profilemul, read_blob, save_map, similarworkspace,
+                   transpose)
 from . import methods  # noqa: F401
 from . import batch  # noqa: F401
 from . import autotune  # noqa: F401

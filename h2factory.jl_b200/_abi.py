@@ -68,6 +68,14 @@ class CoreInfo(C.Structure):
     ]
 
 
+class PassTime(C.Structure):
+    _fields_ = [("pass_", C.c_int32), ("level", C.c_int32), ("milliseconds", C.c_double)]
+
+
+# h2b_pass_time.pass values (H2B_PASS_*)
+PASS_NAMES = {0: "near", 1: "leaf_aggregate", 2: "aggregate", 3: "modulate_in", 4: "i2o",
+              5: "modulate_out", 6: "disaggregate", 7: "leaf_disaggregate"}
+
 LIB_NAME = "libh2b200.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
@@ -77,6 +85,7 @@ EXPORTS = [
     "h2b_workspace_create", "h2b_workspace_destroy", "h2b_matvec", "h2b_matvec_host",
     "h2b_farmul", "h2b_nearmul", "h2b_farmul_noalloc", "h2b_map_blob_write", "h2b_map_blob_read",
     "h2b_core_create_from_blob", "h2b_tensor_wait_timeouts", "h2b_matvec_host_async",
+    "h2b_profile_matvec", "h2b_set_tensor_wait_limit",
 ]
 
 H2B_NOALLOC_SCRATCH_BYTES = 16 << 20
@@ -121,11 +130,13 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.h2b_workspace_create.argtypes = [vp, C.c_int32, C.POINTER(vp)]
     lib.h2b_workspace_destroy.argtypes = [vp]
     lib.h2b_tensor_wait_timeouts.argtypes = [C.c_int32, C.POINTER(C.c_uint32)]
+    lib.h2b_set_tensor_wait_limit.argtypes = [C.c_int32, C.c_uint32]
     mv = [vp, C.c_int32, C.c_int32, vp, C.c_int64, vp, C.c_int64, _f64p, _f64p, vp]
     for name in ("h2b_matvec", "h2b_matvec_host", "h2b_matvec_host_async", "h2b_farmul", "h2b_nearmul"):
         getattr(lib, name).argtypes = mv
     # far part in the library's built-in scratch: takes the core instead of a workspace
     lib.h2b_farmul_noalloc.argtypes = mv
+    lib.h2b_profile_matvec.argtypes = mv + [C.POINTER(PassTime), C.c_int32, C.POINTER(C.c_int32)]
     for name in EXPORTS:
         if name not in ("h2b_version", "h2b_last_error"):
             getattr(lib, name).restype = C.c_int
@@ -141,6 +152,11 @@ def check(status: int) -> None:
         if status == H2B_BUSY:
             raise WorkspaceBusyError(status, msg)
         raise H2BError(status, msg)
+
+
+def set_tensor_wait_limit(limit: int, device: int = 0) -> None:
+    """Bound of the tensor-core kernels' mbarrier waits on `device` (0 restores the default)."""
+    check(load_library().h2b_set_tensor_wait_limit(device, limit))
 
 
 def tensor_wait_timeouts(device: int = 0) -> int:

@@ -24,7 +24,7 @@ from . import _abi
 from .trees import Plans, Tree
 
 __all__ = ["H2Core", "DeviceCore", "H2Workspace", "OrientedMap", "transpose", "adjoint",
-           "mul_", "farmul_", "nearmul_", "similarworkspace", "flatten"]
+           "mul_", "farmul_", "nearmul_", "similarworkspace", "flatten", "profilemul"]
 
 _MODES = {"forward": _abi.H2B_FORWARD, "transpose": _abi.H2B_TRANSPOSE,
           "adjoint": _abi.H2B_ADJOINT}
@@ -501,6 +501,34 @@ class H2Workspace:
         _abi.check(self.lib.h2b_matvec_host_async(self.handle, mode, nrhs, x.ctypes.data_as(C.c_void_p),
                                                   nin, y.ctypes.data_as(C.c_void_p), nout, a, b,
                                                   C.c_void_p(stream)))
+
+
+def profilemul(A, x, y=None, alpha=None, beta=None, stream=None) -> list:
+    """mul! with every pass timed on the device (h2b_profile_matvec), like H2Factory's
+    Diagnostics.profilemul (src/diagnostics/timing.jl:150-160). Returns one record per launch,
+    {"pass", "level", "ms"}, in launch order; `y` receives the product."""
+    import torch
+
+    ws, mode = _split(A)
+    nrow, ncol = ws.shape
+    nout, nin = (nrow, ncol) if mode == _abi.H2B_FORWARD else (ncol, nrow)
+    xp, nrhs, ldx = _colmajor(x, nin)
+    if y is None:
+        y = torch.zeros((nrhs, nout), dtype=x.dtype, device=x.device).t() if x.dim() == 2 else \
+            torch.zeros(nout, dtype=x.dtype, device=x.device)
+    yp, nrhs_y, ldy = _colmajor(y, nout)
+    if nrhs != nrhs_y:
+        raise ValueError("x and y have different numbers of columns")
+    a, b = _alphabeta(alpha, beta)
+    if stream is None:
+        stream = torch.cuda.current_stream(x.device).cuda_stream
+    cap = 256
+    recs = (_abi.PassTime * cap)()
+    count = C.c_int32(0)
+    _abi.check(ws.lib.h2b_profile_matvec(ws.handle, mode, nrhs, C.c_void_p(xp), ldx, C.c_void_p(yp), ldy, a, b,
+                                         C.c_void_p(stream), recs, cap, C.byref(count)))
+    return [{"pass": _abi.PASS_NAMES.get(r.pass_, str(r.pass_)), "level": int(r.level), "ms": float(r.milliseconds)}
+            for r in recs[:min(cap, count.value)]]
 
 
 class OrientedMap:

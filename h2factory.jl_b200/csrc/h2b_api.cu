@@ -141,6 +141,7 @@ struct h2b_workspace {
     void *am = nullptr, *dm = nullptr, *as = nullptr, *ds = nullptr;
     void *xbuf = nullptr, *ybuf = nullptr;  // staging for h2b_matvec_host
     void *xnear = nullptr;  // gathered x rows for the tensor-core near kernel (real, >= 8 RHS)
+    unsigned *timeouts = nullptr;  // pinned: the device's tensor-core wait timeouts before / after a call
     std::atomic<int> busy{0};
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr, ev_far = nullptr;
@@ -1032,6 +1033,16 @@ h2b_status h2b_tensor_wait_timeouts(int32_t device, uint32_t *count) {
     return H2B_OK;
 }
 
+h2b_status h2b_set_tensor_wait_limit(int32_t device, uint32_t limit) {
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(H2B_ERR_INVALID, "device %d not present", device);
+    DeviceGuard guard(device);
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(set_umma_wait_limit(limit));
+    return H2B_OK;
+}
+
 h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **out) {
     if (!desc || !out) return fail(H2B_ERR_INVALID, "null argument");
     *out = nullptr;
@@ -1098,6 +1109,7 @@ h2b_status h2b_workspace_destroy(h2b_workspace *ws) {
     DeviceGuard guard(ws->core->device);
     if (ws->ev_done) cudaEventSynchronize(ws->ev_done);
     for (void *p : ws->allocs) cudaFree(p);
+    if (ws->timeouts) cudaFreeHost(ws->timeouts);
     if (ws->aux) cudaStreamDestroy(ws->aux);
     if (ws->ev_fork) cudaEventDestroy(ws->ev_fork);
     if (ws->ev_join) cudaEventDestroy(ws->ev_join);
@@ -1148,6 +1160,7 @@ h2b_status h2b_workspace_create(h2b_core *core, int32_t max_nrhs, h2b_workspace 
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_far, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ws->ev_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&ws->timeouts, 2 * sizeof(unsigned), cudaHostAllocDefault);
     if (e != cudaSuccess) {
         h2b_workspace_destroy(ws);
         return fail(e == cudaErrorMemoryAllocation ? H2B_ERR_NOMEM : H2B_ERR_CUDA,
@@ -1188,41 +1201,88 @@ h2b_status run_i2o(h2b_core *c, const SideHost &D, const SideHost &A, const FarA
     return H2B_OK;
 }
 
-h2b_status far_passes(h2b_workspace *ws, int mode, int nrhs, const void *x, int64_t ldx, void *y,
-                      int64_t ldy, cdouble alpha_eff, cdouble beta, cudaStream_t st,
-                      cudaEvent_t wait_before_scatter) {
-    h2b_core *c = ws->core;
+// Per-pass device timing (h2b_profile_matvec): after every launch an event is recorded on the
+// pass stream and tagged with the pass and its level; the elapsed time between consecutive events
+// is that launch's duration on the device.
+struct PassTimer {
+    std::vector<cudaEvent_t> ev;
+    std::vector<std::pair<int, int>> tag;  // (operation, level) of the launch ending at ev[i + 1]
+    cudaError_t event(cudaStream_t st) {
+        cudaEvent_t e = nullptr;
+        cudaError_t r = cudaEventCreate(&e);
+        if (r != cudaSuccess) return r;
+        ev.push_back(e);
+        return cudaEventRecord(e, st);
+    }
+    cudaError_t start(cudaStream_t st) { return event(st); }
+    cudaError_t mark(cudaStream_t st, int op, int level) {
+        tag.emplace_back(op, level);
+        return event(st);
+    }
+    ~PassTimer() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+};
+
+#define PASS_MARK(op, lvl)                                    \
+    do {                                                      \
+        if (tm) CUDA_TRY(tm->mark(st, (op), (lvl)));          \
+    } while (0)
+
+// The far passes (farmul!, src/farinteractions/farmul.jl:47-70) on the arenas of `fa`: leaf
+// aggregation, upward transfers, (Toeplitz: forward transforms), I2O, (inverse transforms),
+// downward transfers, leaf disaggregation into y. `wait_before_scatter` (optional) orders the final
+// scatter after other work on y; `tm` (optional) records each launch's device time.
+h2b_status far_passes_fa(h2b_core *c, const FarArgs &fa, const void *x, int64_t ldx, void *y, int64_t ldy,
+                         cdouble alpha_eff, cdouble beta, cudaStream_t st, cudaEvent_t wait_before_scatter,
+                         PassTimer *tm) {
+    const int mode = fa.mode;
     const SideHost &A = mode == H2B_FORWARD ? c->trial : c->test;
     const SideHost &D = mode == H2B_FORWARD ? c->test : c->trial;
     const bool cplx = c->field == H2B_COMPLEX;
     const int pr = c->precision;
-    FarArgs fa{mode, nrhs, ws->am, ws->dm, ws->as, ws->ds};
     const bool conjc = mode == H2B_ADJOINT && c->conj_leaf;
     const bool toep = c->dmap.coupling_kind == H2B_COUPLING_TOEPLITZ;
-    const int maxcoef = std::max(A.maxcoef, D.maxcoef);
-    const int maxt = std::max(A.maxtsize, D.maxtsize);
     CUDA_TRY(launch_leaf_aggregate(cplx, pr, c->dmap, A.d, A.d_agg_leaves, A.n_agg_leaves, A.maxcoef,
                                    conjc, fa, x, ldx, st));
-    for (const Stage &sg : A.agg_inner)
+    PASS_MARK(H2B_PASS_LEAF_AGGREGATE, 0);
+    for (const Stage &sg : A.agg_inner) {
         CUDA_TRY(launch_transfer_up(cplx, pr, c->dmap, A.d, sg.d_nodes, sg.n, mode == H2B_ADJOINT, fa,
                                     A.maxcoef, A.maxsep, st));
-    if (toep)
+        PASS_MARK(H2B_PASS_AGGREGATE, sg.level);
+    }
+    if (toep) {
         CUDA_TRY(launch_toeplitz_in(cplx, pr, c->dmap, A.d, A.d_store, A.n_store, mode == H2B_TRANSPOSE,
                                     fa, A.maxtsize, A.maxaxis, st));
+        PASS_MARK(H2B_PASS_MODULATE_IN, 0);
+    }
     {
         const h2b_status si = run_i2o(c, D, A, fa, st);
         if (si) return si;
+        PASS_MARK(H2B_PASS_I2O, 0);
     }
-    if (toep)
+    if (toep) {
         CUDA_TRY(launch_toeplitz_out(cplx, pr, c->dmap, D.d, D.d_recv, D.n_recv, mode != H2B_TRANSPOSE,
                                      fa, D.maxtsize, D.maxaxis, st));
-    for (const Stage &sg : D.dis_down)
+        PASS_MARK(H2B_PASS_MODULATE_OUT, 0);
+    }
+    for (const Stage &sg : D.dis_down) {
         CUDA_TRY(launch_transfer_down(cplx, pr, c->dmap, D.d, sg.d_nodes, sg.n, D.d_received, fa,
                                       D.maxcoef, D.maxsep, st));
+        PASS_MARK(H2B_PASS_DISAGGREGATE, sg.level);
+    }
     if (wait_before_scatter) CUDA_TRY(cudaStreamWaitEvent(st, wait_before_scatter, 0));
     CUDA_TRY(launch_leaf_disaggregate(cplx, pr, c->dmap, D.d, D.d_init_leaves, D.n_init_leaves, conjc,
                                       fa, alpha_eff, beta, y, ldy, st));
+    PASS_MARK(H2B_PASS_LEAF_DISAGGREGATE, 0);
     return H2B_OK;
+}
+
+h2b_status far_passes(h2b_workspace *ws, int mode, int nrhs, const void *x, int64_t ldx, void *y,
+                      int64_t ldy, cdouble alpha_eff, cdouble beta, cudaStream_t st,
+                      cudaEvent_t wait_before_scatter, PassTimer *tm = nullptr) {
+    const FarArgs fa{mode, nrhs, ws->am, ws->dm, ws->as, ws->ds};
+    return far_passes_fa(ws->core, fa, x, ldx, y, ldy, alpha_eff, beta, st, wait_before_scatter, tm);
 }
 
 cdouble cmul(cdouble a, cdouble b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
@@ -1327,6 +1387,7 @@ static h2b_status matvec_host_impl(h2b_workspace *ws, int32_t mode, int32_t nrhs
     DeviceGuard guard(c->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_done, 0));
+    if (wait) CUDA_TRY(copy_umma_timeouts_async(&ws->timeouts[0], st));
     CUDA_TRY(cudaMemcpy2DAsync(ws->xbuf, nin * vsz, x, ldx * vsz, nin * vsz, nrhs, cudaMemcpyHostToDevice, st));
     const bool need_y = beta && (beta[0] != 0.0 || beta[1] != 0.0);
     if (need_y)
@@ -1336,7 +1397,12 @@ static h2b_status matvec_host_impl(h2b_workspace *ws, int32_t mode, int32_t nrhs
     if (s) return s;
     CUDA_TRY(cudaMemcpy2DAsync(y, ldy * vsz, ws->ybuf, nout * vsz, nout * vsz, nrhs, cudaMemcpyDeviceToHost, st));
     if (wait) {
+        CUDA_TRY(copy_umma_timeouts_async(&ws->timeouts[1], st));
         CUDA_TRY(cudaStreamSynchronize(st));
+        if (ws->timeouts[1] != ws->timeouts[0])
+            return fail(H2B_ERR_CUDA,
+                        "a bounded tensor-core wait gave up during this product (%u on the device so far): some "
+                        "output tiles were not written; see h2b_tensor_wait_timeouts", ws->timeouts[1]);
     } else {
         cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
         CUDA_TRY(cudaStreamIsCapturing(st, &cap));
@@ -1355,6 +1421,55 @@ h2b_status h2b_matvec_host_async(h2b_workspace *ws, int32_t mode, int32_t nrhs, 
                                  int64_t ldx, void *y, int64_t ldy, const double *alpha,
                                  const double *beta, void *stream) {
     return matvec_host_impl(ws, mode, nrhs, x, ldx, y, ldy, alpha, beta, stream, false);
+}
+
+h2b_status h2b_profile_matvec(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x, int64_t ldx,
+                              void *y, int64_t ldy, const double *alpha, const double *beta, void *stream,
+                              h2b_pass_time *records, int32_t capacity, int32_t *count) {
+    if (!ws || !x || !y || !count || (capacity > 0 && !records)) return fail(H2B_ERR_INVALID, "null argument");
+    if (mode < 0 || mode > 2) return fail(H2B_ERR_INVALID, "mode must be 0, 1 or 2");
+    if (nrhs < 1 || nrhs > ws->max_nrhs)
+        return fail(H2B_ERR_INVALID, "nrhs = %d outside 1..%d (workspace max_nrhs)", nrhs, ws->max_nrhs);
+    if ((alpha == nullptr) != (beta == nullptr))
+        return fail(H2B_ERR_INVALID, "alpha and beta must both be given or both be NULL");
+    h2b_core *c = ws->core;
+    const int64_t nout = mode == H2B_FORWARD ? c->test.ndofs : c->trial.ndofs;
+    const int64_t nin = mode == H2B_FORWARD ? c->trial.ndofs : c->test.ndofs;
+    if (ldx < nin || ldy < nout) return fail(H2B_ERR_INVALID, "leading dimension smaller than the vector length");
+    if (c->field == H2B_REAL && alpha && (alpha[1] != 0.0 || beta[1] != 0.0))
+        return fail(H2B_ERR_INVALID, "complex alpha/beta on a real map");
+    BusyGuard busy(ws->busy);
+    if (!busy.ok) return fail(H2B_BUSY, "workspace is in use by another call");
+    DeviceGuard guard(c->device);
+    (void)cudaGetLastError();  // a non-sticky error left by other code is not this call's
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(H2B_ERR_INVALID, "h2b_profile_matvec waits for its events and cannot run inside a stream capture");
+    CUDA_TRY(cudaStreamWaitEvent(st, ws->ev_done, 0));
+    const cdouble a = alpha ? cdouble{alpha[0], alpha[1]} : cdouble{1.0, 0.0};
+    const cdouble b = beta ? cdouble{beta[0], beta[1]} : cdouble{0.0, 0.0};
+    PassTimer tm;
+    CUDA_TRY(tm.start(st));
+    // the passes of h2b_matvec, serialised on the caller's stream so that each has its own interval
+    CUDA_TRY(launch_near(c->field == H2B_COMPLEX, mode, c->dnear, c->test.d, c->trial.d, nrhs, x, ldx, y, ldy,
+                         a, b, ws->xnear, st));
+    CUDA_TRY(tm.mark(st, H2B_PASS_NEAR, 0));
+    const h2b_status s = far_passes(ws, mode, nrhs, x, ldx, y, ldy, cmul(c->alpha[mode], a), cdouble{1.0, 0.0},
+                                    st, nullptr, &tm);
+    if (s) return s;
+    CUDA_TRY(cudaEventRecord(ws->ev_done, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *count = (int32_t)tm.tag.size();
+    for (size_t i = 0; i < tm.tag.size() && (int32_t)i < capacity; ++i) {
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, tm.ev[i], tm.ev[i + 1]));
+        records[i].pass = tm.tag[i].first;
+        records[i].level = tm.tag[i].second;
+        records[i].milliseconds = ms;
+    }
+    return H2B_OK;
 }
 
 }  // extern "C"
@@ -1394,41 +1509,6 @@ h2b_status noalloc_scratch(void **out) {
 namespace {
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
-
-// The far passes of far_passes() with the arenas given in `fa` (no workspace, caller's stream).
-h2b_status far_passes_scratch(h2b_core *c, const FarArgs &fa, const void *x, int64_t ldx, void *y,
-                              int64_t ldy, cdouble alpha_eff, cdouble beta, cudaStream_t st) {
-    const int mode = fa.mode;
-    const SideHost &A = mode == H2B_FORWARD ? c->trial : c->test;
-    const SideHost &D = mode == H2B_FORWARD ? c->test : c->trial;
-    const bool cplx = c->field == H2B_COMPLEX;
-    const int pr = c->precision;
-    const bool conjc = mode == H2B_ADJOINT && c->conj_leaf;
-    const bool toep = c->dmap.coupling_kind == H2B_COUPLING_TOEPLITZ;
-    const int maxcoef = std::max(A.maxcoef, D.maxcoef);
-    const int maxt = std::max(A.maxtsize, D.maxtsize);
-    CUDA_TRY(launch_leaf_aggregate(cplx, pr, c->dmap, A.d, A.d_agg_leaves, A.n_agg_leaves, A.maxcoef,
-                                   conjc, fa, x, ldx, st));
-    for (const Stage &sg : A.agg_inner)
-        CUDA_TRY(launch_transfer_up(cplx, pr, c->dmap, A.d, sg.d_nodes, sg.n, mode == H2B_ADJOINT, fa,
-                                    A.maxcoef, A.maxsep, st));
-    if (toep)
-        CUDA_TRY(launch_toeplitz_in(cplx, pr, c->dmap, A.d, A.d_store, A.n_store, mode == H2B_TRANSPOSE,
-                                    fa, A.maxtsize, A.maxaxis, st));
-    {
-        const h2b_status si = run_i2o(c, D, A, fa, st);
-        if (si) return si;
-    }
-    if (toep)
-        CUDA_TRY(launch_toeplitz_out(cplx, pr, c->dmap, D.d, D.d_recv, D.n_recv, mode != H2B_TRANSPOSE,
-                                     fa, D.maxtsize, D.maxaxis, st));
-    for (const Stage &sg : D.dis_down)
-        CUDA_TRY(launch_transfer_down(cplx, pr, c->dmap, D.d, sg.d_nodes, sg.n, D.d_received, fa,
-                                      D.maxcoef, D.maxsep, st));
-    CUDA_TRY(launch_leaf_disaggregate(cplx, pr, c->dmap, D.d, D.d_init_leaves, D.n_init_leaves, conjc,
-                                      fa, alpha_eff, beta, y, ldy, st));
-    return H2B_OK;
-}
 
 }  // namespace
 
@@ -1473,8 +1553,8 @@ extern "C" h2b_status h2b_farmul_noalloc(const h2b_core *core_in, int32_t mode, 
     const cdouble aA = c->alpha[mode];
     if (!alpha) {
         CUDA_TRY(launch_zero_columns(cplx, nrhs, nout, y, ldy, st));
-        return far_passes_scratch(c, fa, x, ldx, y, ldy, aA, cdouble{0.0, 0.0}, st);
+        return far_passes_fa(c, fa, x, ldx, y, ldy, aA, cdouble{0.0, 0.0}, st, nullptr, nullptr);
     }
-    return far_passes_scratch(c, fa, x, ldx, y, ldy, cmul(aA, cdouble{alpha[0], alpha[1]}),
-                              cdouble{beta[0], beta[1]}, st);
+    return far_passes_fa(c, fa, x, ldx, y, ldy, cmul(aA, cdouble{alpha[0], alpha[1]}),
+                         cdouble{beta[0], beta[1]}, st, nullptr, nullptr);
 }

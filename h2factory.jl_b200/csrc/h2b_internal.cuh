@@ -182,6 +182,10 @@ cudaError_t launch_i2o_umma(bool cplx, const DMap &m, const DSide &recv, const D
                             int nnodes, const FarArgs &fa, int maxcoef, cudaStream_t st);
 // mbarrier waits of the tensor-core kernels that gave up on the current device (0 in a healthy run)
 cudaError_t read_umma_timeouts(unsigned *count);
+// the same count copied to host memory in order on `st`
+cudaError_t copy_umma_timeouts_async(unsigned *host, cudaStream_t st);
+// try_wait attempts of every bounded mbarrier wait on the current device (0: the default)
+cudaError_t set_umma_wait_limit(unsigned limit);
 cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const DSide &recv,
                                 const SibGroups &g, int maxslen, const FarArgs &fa, cudaStream_t st);
 cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const DSide &s,

@@ -6,28 +6,35 @@
 // of i2oprotocol.jl:87-92). For one receiver this is one GEMM whose K dimension runs over the
 // concatenated pairs: D[nc x nq] = [op(B_1) op(B_2) ...] [m_1; m_2; ...].
 //
-// One CTA per (receiver, 128-row tile of its coefficients, tile of right-hand sides), two CTAs per
-// SM. The K dimension streams in chunks of 16 FP32 values: every thread copies its share of chunk
-// c + 3 from global memory (L2-resident couplings and moments) into a 4-stage ring of raw shared
-// buffers with cp.async (gathers and zero fill included), so three chunks are in flight without
-// registers; a split pass turns raw chunk c into the canonical no-swizzle K-major layout of the
-// tensor cores, each FP32 value as a TF32 high part and a TF32 remainder; one thread issues per
-// 8-wide k step the three products hi*hi + hi*lo + lo*hi (the lo*lo term is below FP32 rounding)
-// into an FP32 accumulator in tensor memory, and a commit to an mbarrier per split buffer releases
-// it, so splitting chunk c + 1 overlaps the products of chunk c. Accumulators live for 8 chunks (48
-// MMAs) only: two alternate, and each finished one is added into an FP64 sum kept in tensor memory,
-// because every MMA rounds its accumulator toward zero (one accumulator through a whole interaction
-// list, ~30,000 MMAs, measured 1e-4 relative error; segments keep it near FP32 rounding). The
-// epilogue reads the sums with tcgen05.ld and stores the FP32 moments.
+// One CTA per (receiver, 128-row tile of its coefficients, tile of right-hand sides), one CTA per
+// SM, warp-specialised; the K dimension streams in chunks of 16 FP32 values and every hand-off is
+// an mbarrier (no block barrier inside the loop):
+//   * coupling warps (0-3), one thread per tile row: load the row's 16 values of chunk c + 3 into
+//     a register ring (the couplings are L2-resident), split chunk c into TF32 high parts and
+//     rounded remainders and write them into a tensor-memory stage with tcgen05.st. The MMAs take
+//     this operand (A) straight from tensor memory, so it never passes through shared memory;
+//   * moment warps (4-7): cp.async each chunk's source moments (B) into a shared-memory stage of
+//     an 8-deep ring in the canonical no-swizzle K-major layout, then split their own elements in
+//     place into TF32 high parts plus a remainder buffer;
+//   * one MMA thread (warp 12): per 8-wide k step the products hi*hi + hi*lo + lo*hi (the lo*lo
+//     term is below FP32 rounding) into an FP32 accumulator in tensor memory; commits release the
+//     operand stages;
+//   * drain warps (8-11): the tensor cores round each accumulation toward zero, so one FP32
+//     accumulator over a whole interaction list loses ~1e-4; accumulators live for 8 chunks only,
+//     two alternate, and each finished one is added into an FP64 sum in tensor memory, which the
+//     epilogue rounds once into the FP32 moments.
 //
-// Complex maps run as real GEMMs: with B = Br + i Bi and m = mr + i mi,
-//   [Re l | Im l] = [Br Bi] (interleaved along k) x [[mr, mi]; [-mi, mr]] (interleaved rows),
-// so the coupling's interleaved (re, im) storage is the A operand as it lies in memory and each
-// moment value feeds two B rows. Adjoint maps conjugate B in the split pass; symmetry-reduced
-// couplings apply their row / column permutations in the copy addresses.
+// Complex maps run as real GEMMs without expanding the moments: with a = op(B)[i, k] and the
+// moments interleaved (re, im) along k as they lie in memory,
+//   Re l = sum_k [ar, -ai] . [mr, mi],   Im l = sum_k [ai, ar] . [mr, mi],
+// so the coupling warps write two A operands (A_re = (ar, -ai), A_im = (ai, ar) per k) and every
+// B chunk feeds both accumulators. Adjoint maps conjugate a; symmetry-reduced couplings apply
+// their row / column permutations in the load addresses.
 //
 // Every wait on an mbarrier is bounded: a wait that gives up counts itself in a device counter
-// (h2b_tensor_wait_timeouts), the CTA stops issuing, frees its tensor memory and returns.
+// (h2b_tensor_wait_timeouts) and sets the CTA's abort flag; every role then leaves its loop, the
+// MMA thread waits (with the full bound) for the products it issued, the moment warps for their
+// copies, and the CTA frees its tensor memory and returns with its output tile unwritten.
 
 #include "h2b_internal.cuh"
 
@@ -35,22 +42,24 @@ namespace h2b {
 
 namespace {
 
-constexpr int UM_M = 128;        // output rows per tile = tensor-memory lanes
-constexpr int UM_KC = 16;        // FP32 K values per chunk: 4 groups of 16 bytes per row
+constexpr int UM_M = 128;         // output rows per tile = tensor-memory lanes
+constexpr int UM_KC = 16;         // FP32 K values per chunk: 4 groups of 16 bytes per B row
 constexpr int UM_KG = UM_KC / 4;
-constexpr int UM_THREADS = 256;
-constexpr int UM_NT_MAX = 64;    // MMA N (FP32 accumulator columns) per tile, at most
-constexpr int UM_SEG = 8;        // chunks (48 MMAs) per accumulation segment
-constexpr int UM_RS = 4;         // raw stages: chunks c + 1 .. c + 3 in flight while c is split
-constexpr uint32_t UM_LBO = 128;           // bytes between the two 16-byte K halves of a k step
-constexpr uint32_t UM_SBO = UM_KG * 128;   // bytes between 8-row groups (4 groups of 128 bytes)
-constexpr uint32_t UM_AHALF = UM_M * UM_KC * 4;  // bytes of one A split part (8 KB)
-constexpr uint32_t UM_RAWROW = UM_KC * 4 + 16;   // raw row layout: 64 bytes + 16 of padding
-constexpr uint32_t UM_RAWA = UM_M * UM_RAWROW;   // raw A bytes (>= the column layouts' 8,448)
-constexpr unsigned UM_SPIN = 1u << 22;           // try_wait attempts before a wait gives up
-constexpr int UM_XMAP = 512;     // moment-row permutations up to this length are read from shared memory
+constexpr int UM_NA = 4;          // coupling stages in tensor memory
+constexpr int UM_NB = 8;          // moment stages in shared memory
+constexpr int UM_LAG = UM_NB - 2; // moment copies issued this many chunks ahead of the split
+constexpr int UM_SEG = 8;         // chunks per accumulation segment
+constexpr int UM_WARPS = 13;      // 4 coupling, 4 moment, 4 drain, 1 MMA
+constexpr int UM_THREADS = UM_WARPS * 32;
+constexpr int UM_NT_MAX_REAL = 64;    // MMA N (right-hand sides) per tile, real maps
+constexpr int UM_NT_MAX_CPLX = 32;    // complex maps (two accumulators: Re and Im)
+constexpr uint32_t UM_LBO = 128;            // bytes between the two 16-byte K halves of a k step
+constexpr uint32_t UM_SBO = UM_KG * 128;    // bytes between 8-row groups (4 groups of 128 bytes)
+constexpr unsigned UM_SPIN = 1u << 22;      // default try_wait attempts before a wait gives up
+constexpr unsigned UM_SPIN_FINAL = 1u << 26;  // the final wait for products already issued
 
 __device__ unsigned int g_umma_timeouts = 0;
+__device__ unsigned int g_umma_wait_limit = UM_SPIN;
 
 __device__ __forceinline__ int um_ncoef(const DSide &s, int lvl) {
     return s.shape[3 * lvl] * s.shape[3 * lvl + 1] * s.shape[3 * lvl + 2];
@@ -86,22 +95,20 @@ __device__ __forceinline__ uint32_t tf32_bits(float a) {
     return (__float_as_uint(a) + 0x1000u) & 0xFFFFE000u;
 }
 
-// v = hi + lo with hi, lo TF32: the high part and the rounded remainder
-__device__ __forceinline__ void st_split(uint32_t hi_addr, uint32_t lo_addr, float a, float b, float c, float d) {
-    const uint32_t h0 = tf32_bits(a), h1 = tf32_bits(b), h2 = tf32_bits(c), h3 = tf32_bits(d);
-    const uint32_t l0 = tf32_bits(a - __uint_as_float(h0)), l1 = tf32_bits(b - __uint_as_float(h1));
-    const uint32_t l2 = tf32_bits(c - __uint_as_float(h2)), l3 = tf32_bits(d - __uint_as_float(h3));
-    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(hi_addr), "r"(h0), "r"(h1), "r"(h2), "r"(h3));
-    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(lo_addr), "r"(l0), "r"(l1), "r"(l2), "r"(l3));
+// x = hi + lo with hi, lo TF32: the high part and the rounded remainder
+__device__ __forceinline__ void split2(float x, uint32_t &hi, uint32_t &lo) {
+    hi = tf32_bits(x);
+    lo = tf32_bits(x - __uint_as_float(hi));
 }
 
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
-                                          uint32_t accumulate) {
+// D (+)= A (tensor memory) * B (shared memory), kind::tf32
+__device__ __forceinline__ void umma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc,
+                                        uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -109,10 +116,19 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                  : "memory");
 }
 
-// bounded wait for the completion of the mbarrier phase with the given parity
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(bar)) : "memory");
+}
+
+// bounded wait for the completion of the mbarrier phase with the given parity; false when it gave
+// up (counted in g_umma_timeouts)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned limit) {
     const uint32_t a = su32(bar);
-    for (unsigned it = 0; it < UM_SPIN; ++it) {
+    for (unsigned it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -127,15 +143,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return false;
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-        "%14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// the same wait taken by a whole warp, with one outcome for all its lanes (the warps that go on to
+// warp-collective tcgen05.ld / tcgen05.st must not diverge)
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, unsigned limit) {
+    const bool ok = mbar_wait(bar, parity, limit);
+    return __all_sync(0xffffffffu, ok);
 }
+
+__device__ __forceinline__ bool warp_aborted(volatile int *flag) { return __any_sync(0xffffffffu, *flag != 0); }
 
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
     asm volatile(
@@ -146,18 +161,26 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
         : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-    uint32_t r[8];
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
                    "=r"(r[7])
                  : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = __uint_as_float(r[u]);
 }
 
-// element copy global -> shared; src_bytes 0 writes zeros (src is then not read)
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// element copy global -> shared; ok = false writes zeros (src is then not read)
 template <int EB>
 __device__ __forceinline__ void cp_elem(uint32_t dst, const void *src, bool ok) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(EB), "r"(ok ? EB : 0)
@@ -176,32 +199,58 @@ template <> struct UmScalar<cfloat> {
     static constexpr int W = 2;
 };
 
-// The operands of one pair: op(B)[i, k] and the source moment rows, with the permutations of a
-// symmetry-reduced coupling (sets [rowperm | rowperm^-1 | colperm | colperm^-1]) resolved.
+// The operands of one pair with the permutations of a symmetry-reduced coupling (sets
+// [rowperm | rowperm^-1 | colperm | colperm^-1]) resolved.
 template <class T>
 struct UmPair {
-    const T *B;   // coupling block
-    const T *X;   // source moments, column-major snc x nq
-    int snc;      // source coefficients
-    int nk;       // K chunks
+    const T *B;         // coupling block
+    const T *X;         // source moments of the tile's first right-hand side, column-major snc x nq
+    int snc;            // source coefficients
+    int nk;             // K chunks
     const int *rowmap;  // output row -> row (forward) / column (transposed) of B, or null
     const int *xmap;    // k -> source moment row, or null
 };
 
+template <class T>
+__device__ __forceinline__ UmPair<T> um_pair(const DMap &m, const DSide &r, const DSide &t, int p, int nc,
+                                             bool fwd, int nrhs, int q0, const T *am) {
+    constexpr int W = UmScalar<T>::W;
+    UmPair<T> u;
+    u.snc = um_ncoef(t, t.level[r.i2o_src[p]]);
+    u.nk = (W * u.snc + UM_KC - 1) / UM_KC;
+    u.B = static_cast<const T *>(m.cpl) + r.pair_cpl[p];
+    u.X = am + r.pair_src[p] * nrhs + (int64_t)q0 * u.snc;
+    const int64_t ps = r.pair_perm ? r.pair_perm[p] : -1;
+    u.rowmap = nullptr;
+    u.xmap = nullptr;
+    if (ps >= 0) {
+        if (fwd) {  // t[rp[i], cp[j]] = M[i, j]: out[i] += sum_j M[rp^-1[i], j] x[cp[j]]
+            u.rowmap = m.perm + ps + nc;
+            u.xmap = m.perm + ps + 2 * nc;
+        } else {    // out[j] += sum_i op(M)[cp^-1[j], i] x[rp[i]]
+            u.rowmap = m.perm + ps + 3 * u.snc;
+            u.xmap = m.perm + ps;
+        }
+    }
+    return u;
+}
+
+__device__ __forceinline__ float2 ldg2(const cfloat *p) { return __ldg(reinterpret_cast<const float2 *>(p)); }
+
 }  // namespace
 
 template <class T>
-__global__ void __launch_bounds__(UM_THREADS)
+__global__ void __maxnreg__(152)
 i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mode, int nrhs, int qt_max,
                 const T *__restrict__ am, T *__restrict__ dm) {
     constexpr int W = UmScalar<T>::W;
-    constexpr int EB = sizeof(T);        // bytes per element (4 real, 8 complex)
     constexpr int KQ = UM_KC / W;        // elements along k per chunk
     extern __shared__ __align__(128) unsigned char um_smem[];
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t a_full[UM_NA], a_empty[UM_NA], b_full[UM_NB], b_empty[UM_NB];
+    __shared__ uint64_t acc_full[2], acc_empty[2], fin;
     __shared__ uint32_t tmem_slot;
     __shared__ int nchunks_s;
-    __shared__ int xmap_s[UM_XMAP];  // the copied pair's moment-row permutation
+    __shared__ volatile int abort_s;
 
     const int node = nodes[blockIdx.x];
     const int nc = um_ncoef(r, r.level[node]);
@@ -211,12 +260,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     if (m0 >= nc || q0 >= nq) return;  // whole CTA, before any barrier
     const int mt = min(UM_M, nc - m0);
     const int qt = min(qt_max, nq - q0);
-    const int nt = ((W * qt + 15) / 16) * 16;                 // MMA N of this tile
-    const int ntmax = ((W * qt_max + 15) / 16) * 16;          // B rows a split buffer holds
-    const int lb = W == 1 ? nt : ((qt + 7) / 8) * 8;          // B rows copied per chunk
-    const int lbmax = W == 1 ? ntmax : ((qt_max + 7) / 8) * 8;
-    const uint32_t split_bytes = 2 * UM_AHALF + 2u * (uint32_t)ntmax * (UM_KC * 4);
-    const uint32_t raw_bytes = UM_RAWA + (uint32_t)lbmax * UM_RAWROW;
+    const int np = ((qt_max + 15) / 16) * 16;      // MMA N of every tile (zero rows past qt)
     const int p0 = r.i2o_ptr[node], p1 = r.i2o_ptr[node + 1];
     T *out = dm + r.mom_off[node] * nrhs;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -225,11 +269,16 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
         return;
     }
     const bool fwd = mode == H2B_FORWARD, adj = mode == H2B_ADJOINT;
-    const T *B0 = static_cast<const T *>(m.cpl);
+    const unsigned limit = g_umma_wait_limit;
 
-    // tensor memory: two FP32 accumulators of ntmax columns (segments alternate between them) and
-    // the FP64 sum of the drained segments (two columns per value), rounded up to a power of two
-    const uint32_t ncols = ntmax <= 16 ? 64u : (ntmax <= 32 ? 128u : 256u);
+    // tensor memory: two accumulators of W * np columns (segments alternate between them), the
+    // FP64 sum (two columns per value), then UM_NA coupling stages of 32 * W columns (hi, lo)
+    const uint32_t acc_cols = (uint32_t)(W * np);
+    const uint32_t col_master = 2 * acc_cols;
+    const uint32_t col_a = 4 * acc_cols;
+    const uint32_t a_stage_cols = 32u * W;
+    const uint32_t need = col_a + UM_NA * a_stage_cols;
+    const uint32_t ncols = need <= 64 ? 64u : (need <= 128 ? 128u : (need <= 256 ? 256u : 512u));
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_slot)),
                      "r"(ncols)
@@ -237,36 +286,27 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[1])) : "memory");
+        for (int s = 0; s < UM_NA; ++s) {
+            mbar_init(&a_full[s], 128);
+            mbar_init(&a_empty[s], 1);
+        }
+        for (int s = 0; s < UM_NB; ++s) {
+            mbar_init(&b_full[s], 128);
+            mbar_init(&b_empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 128);
+        }
+        mbar_init(&fin, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         nchunks_s = 0;
+        abort_s = 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-
-    auto pair_at = [&](int p) {
-        UmPair<T> u;
-        u.snc = um_ncoef(t, t.level[r.i2o_src[p]]);
-        u.nk = (W * u.snc + UM_KC - 1) / UM_KC;
-        u.B = B0 + r.pair_cpl[p];
-        u.X = am + r.pair_src[p] * nrhs + (int64_t)q0 * u.snc;
-        const int64_t ps = r.pair_perm ? r.pair_perm[p] : -1;
-        u.rowmap = nullptr;
-        u.xmap = nullptr;
-        if (ps >= 0) {
-            if (fwd) {  // t[rp[i], cp[j]] = M[i, j]: out[i] += sum_j M[rp^-1[i], j] x[cp[j]]
-                u.rowmap = m.perm + ps + nc;
-                u.xmap = m.perm + ps + 2 * nc;
-            } else {    // out[j] += sum_i op(M)[cp^-1[j], i] x[rp[i]]
-                u.rowmap = m.perm + ps + 3 * u.snc;
-                u.xmap = m.perm + ps;
-            }
-        }
-        return u;
-    };
     {  // chunks of the whole interaction list
         int mine = 0;
         for (int p = p0 + tid; p < p1; p += UM_THREADS) mine += (W * um_ncoef(t, t.level[r.i2o_src[p]]) + UM_KC - 1) / UM_KC;
@@ -274,292 +314,286 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
         __syncthreads();
     }
     const int C = nchunks_s;
-
-    // Copy mappings. A, forward blocks (column-major, rows contiguous): thread = one tile row,
-    // consecutive lanes consecutive rows, raw layout [k][row]. A, transposed blocks (rows
-    // contiguous along k) and B (moment columns contiguous along k): a warp covers 8 rows x 4
-    // consecutive k, raw layout [row][k] with 80-byte rows. The tile rows a thread copies are
-    // fixed, so a permuted block's row map is read once per pair.
-    const int arow_f = tid & (UM_M - 1);                       // forward: the thread's row
-    const int arow_t0 = (warp & 7) * 8 + (lane & 7);           // transposed: rows arow_t0, + 64
-    const uint32_t colstride = UM_M * EB + 16;                 // raw column layout: bytes per k
-    // copy cursor: pair pp, its chunk pk, chunks issued; the next pair's operands and row map are
-    // fetched a pair ahead (their loads complete while the current pair streams), and a permuted
-    // pair's moment-row map is staged in shared memory once per pair
-    int pp = p0, pk = 0, issued = 0;
-    UmPair<T> pu = pair_at(p0), pn = pu;
-    int hrow[2], hrow_n[2];
-    auto rows_of = [&](const UmPair<T> &u, int (&h)[2]) {
-        if (fwd) {
-            h[0] = arow_f < mt ? (u.rowmap ? u.rowmap[m0 + arow_f] : m0 + arow_f) : 0;
-            h[1] = 0;
-        } else {
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int rr = arow_t0 + 64 * e;
-                h[e] = rr < mt ? (u.rowmap ? u.rowmap[m0 + rr] : m0 + rr) : 0;
-            }
-        }
-    };
-    auto fill_xmap = [&]() {  // every thread calls it (one barrier)
-        if (pu.xmap && pu.snc <= UM_XMAP)
-            for (int k = tid; k < pu.snc; k += UM_THREADS) xmap_s[k] = pu.xmap[k];
-        __syncthreads();
-    };
-    rows_of(pu, hrow);
-    if (p0 + 1 < p1) {
-        pn = pair_at(p0 + 1);
-        rows_of(pn, hrow_n);
-    }
-    fill_xmap();
+    const int G = (C + UM_SEG - 1) / UM_SEG;
+    const uint32_t b_stage_bytes = 2u * (uint32_t)np * (UM_KC * 4);  // hi then lo
     const uint32_t smem0 = su32(um_smem);
-    const uint32_t raw0 = smem0 + 2 * split_bytes;
-    auto issue = [&]() {  // copies of the next chunk into raw stage (issued % UM_RS); one group
-        if (issued < C) {
-            const uint32_t ra = raw0 + (uint32_t)(issued % UM_RS) * raw_bytes, rb = ra + UM_RAWA;
-            const int kq0 = pk * KQ;
-            if (fwd) {
+
+    if (warp < 4) {
+        // ---------------- coupling warps: A operand into tensor memory ----------------
+        const int row = 32 * warp + lane;   // tile row = tensor-memory lane
+        const bool live = row < mt;
+        const uint32_t tl = tmem + ((uint32_t)(32 * warp) << 16);
+        // load cursor: pair lp, chunk lk, the pair's operands and this thread's row of B
+        int lp = p0, lk = 0;
+        UmPair<T> lu = um_pair<T>(m, r, t, p0, nc, fwd, nrhs, q0, am);
+        int brow = live ? (lu.rowmap ? lu.rowmap[m0 + row] : m0 + row) : 0;
+        float ra[4][UM_KC];
+        auto load = [&](float (&v)[UM_KC]) {
+            const int k0 = lk * KQ;
+            if constexpr (W == 2) {
 #pragma unroll
-                for (int j = 0; j < KQ / 2; ++j) {
-                    const int kq = (tid >> 7) + 2 * j, k = kq0 + kq;
-                    const bool ok = arow_f < mt && k < pu.snc;
-                    cp_elem<EB>(ra + (uint32_t)kq * colstride + (uint32_t)arow_f * EB,
-                                ok ? pu.B + hrow[0] + (int64_t)k * nc : pu.B, ok);
+                for (int j = 0; j < KQ; ++j) {
+                    const int k = k0 + j;
+                    float2 x = make_float2(0.f, 0.f);
+                    if (live && k < lu.snc)
+                        x = fwd ? ldg2(lu.B + brow + (int64_t)k * nc) : ldg2(lu.B + k + (int64_t)brow * lu.snc);
+                    v[2 * j] = x.x;
+                    v[2 * j + 1] = x.y;
                 }
             } else {
 #pragma unroll
-                for (int j = 0; j < KQ / 2; ++j) {
-                    const int row = arow_t0 + 64 * (j & 1), kq = (j >> 1) * 4 + (lane >> 3), k = kq0 + kq;
-                    const bool ok = row < mt && k < pu.snc;
-                    cp_elem<EB>(ra + (uint32_t)row * UM_RAWROW + (uint32_t)kq * EB,
-                                ok ? pu.B + k + (int64_t)hrow[j & 1] * pu.snc : pu.B, ok);
+                for (int j = 0; j < KQ; ++j) {
+                    const int k = k0 + j;
+                    float x = 0.f;
+                    if (live && k < lu.snc)
+                        x = fwd ? __ldg(lu.B + brow + (int64_t)k * nc) : __ldg(lu.B + k + (int64_t)brow * lu.snc);
+                    v[j] = x;
                 }
             }
-            const int nrb = lb >> 3;
-            for (int e = tid; e < lb * KQ; e += UM_THREADS) {
-                const int w = e >> 5, l = e & 31;
-                const int q = (w % nrb) * 8 + (l & 7), kq = (w / nrb) * 4 + (l >> 3), k = kq0 + kq;
-                const bool ok = q < qt && k < pu.snc;
-                const T *src = pu.X;
-                if (ok)
-                    src = pu.X + (int64_t)q * pu.snc +
-                          (pu.xmap ? (pu.snc <= UM_XMAP ? xmap_s[k] : pu.xmap[k]) : k);
-                cp_elem<EB>(rb + (uint32_t)q * UM_RAWROW + (uint32_t)kq * EB, src, ok);
-            }
-            ++issued;
-            if (++pk == pu.nk) {
-                pk = 0;
-                if (++pp < p1) {
-                    pu = pn;
-                    hrow[0] = hrow_n[0];
-                    hrow[1] = hrow_n[1];
-                    if (pp + 1 < p1) {
-                        pn = pair_at(pp + 1);
-                        rows_of(pn, hrow_n);
-                    }
-                    __syncthreads();  // every thread's copies read the previous pair's map
-                    fill_xmap();
+            if (++lk == lu.nk) {
+                lk = 0;
+                if (++lp < p1) {
+                    lu = um_pair<T>(m, r, t, lp, nc, fwd, nrhs, q0, am);
+                    brow = live ? (lu.rowmap ? lu.rowmap[m0 + row] : m0 + row) : 0;
                 }
-            }
-        }
-        cp_commit_group();
-    };
-    // raw chunk -> split buffer: TF32 hi / lo in the canonical layout (A conjugated for adjoint maps)
-    auto split = [&](uint32_t ra, uint32_t sbase) {
-        const uint32_t rb = ra + UM_RAWA;
-        const uint32_t ahi = sbase, alo = sbase + UM_AHALF;
-        const uint32_t bhi = sbase + 2 * UM_AHALF, blo = bhi + (uint32_t)ntmax * (UM_KC * 4);
-#pragma unroll
-        for (int j = 0; j < UM_M * UM_KG / UM_THREADS; ++j) {
-            const int g = tid + UM_THREADS * j;
-            int row, kg;
-            float v[4];
-            if (fwd) {
-                row = g & (UM_M - 1);
-                kg = g >> 7;
-                if constexpr (W == 1) {
-#pragma unroll
-                    for (int e = 0; e < 4; ++e)
-                        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v[e]) : "r"(ra + (uint32_t)(4 * kg + e) * colstride + (uint32_t)row * 4));
-                } else {
-#pragma unroll
-                    for (int e = 0; e < 2; ++e)
-                        asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
-                                     : "=f"(v[2 * e]), "=f"(v[2 * e + 1])
-                                     : "r"(ra + (uint32_t)(2 * kg + e) * colstride + (uint32_t)row * 8));
-                }
-            } else {
-                const int w = g >> 5, l = g & 31;
-                row = (w & 15) * 8 + (l & 7);
-                kg = (w >> 4) * 4 + (l >> 3);
-                asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                             : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
-                             : "r"(ra + (uint32_t)row * UM_RAWROW + (uint32_t)kg * 16));
-            }
-            if (W == 2 && adj) {
-                v[1] = -v[1];
-                v[3] = -v[3];
-            }
-            const uint32_t o = goff(row, kg);
-            st_split(ahi + o, alo + o, v[0], v[1], v[2], v[3]);
-        }
-        for (int g = tid; g < lb * UM_KG; g += UM_THREADS) {
-            const int q = g >> 2, kg = g & 3;
-            float v[4];
-            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                         : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
-                         : "r"(rb + (uint32_t)q * UM_RAWROW + (uint32_t)kg * 16));
-            if constexpr (W == 1) {
-                const uint32_t o = goff(q, kg);
-                st_split(bhi + o, blo + o, v[0], v[1], v[2], v[3]);
-            } else if (q < qt) {
-                // row q: (mr, -mi) per k feeds Re; row qt + q: (mi, mr) feeds Im
-                const uint32_t o1 = goff(q, kg), o2 = goff(qt + q, kg);
-                st_split(bhi + o1, blo + o1, v[0], -v[1], v[2], -v[3]);
-                st_split(bhi + o2, blo + o2, v[1], v[0], v[3], v[2]);
-            }
-        }
-    };
-
-    // The tensor cores round each MMA's sum toward zero, so one FP32 accumulator carried through
-    // thousands of MMAs loses ~1e-4 of its value. Chunks are therefore summed in segments of
-    // UM_SEG chunks, alternating between two accumulators; each finished segment is added into an
-    // FP64 running sum in tensor memory while the next one is on the tensor cores.
-    const int lq = warp & 3, half = warp >> 2;  // warp w reads lanes 32 (w % 4) .. + 31
-    const int row = 32 * lq + lane;
-    const uint32_t tlane = tmem + ((uint32_t)(32 * lq) << 16);
-    const uint32_t tmaster = tlane + 2u * (uint32_t)ntmax;
-    auto drain = [&](int a, bool first) {  // master (+)= accumulator a, over this warp's half
-        const int hw = ntmax / 2;
-        for (int j0 = half * hw; j0 < (half + 1) * hw && j0 < nt; j0 += 8) {
-            float v[8];
-            tmem_ld8(tlane + (uint32_t)(a * ntmax + j0), v);
-            uint32_t w[16];
-            if (!first) tmem_ld16(tmaster + 2u * (uint32_t)j0, w);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const double mv = (first ? 0.0 : __hiloint2double((int)w[2 * u + 1], (int)w[2 * u])) + (double)v[u];
-                w[2 * u] = (uint32_t)__double2loint(mv);
-                w[2 * u + 1] = (uint32_t)__double2hiint(mv);
-            }
-            tmem_st16(tmaster + 2u * (uint32_t)j0, w);
-        }
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-    };
-
-    const uint32_t idesc = tf32_idesc(UM_M, nt);
-#pragma unroll
-    for (int s = 0; s < UM_RS - 1; ++s) issue();
-    int c = 0;
-    bool bad = false;
-    for (; c < C; ++c) {
-        const int s = c & 1, g = c / UM_SEG, a = g & 1;
-        const uint32_t sbase = smem0 + (uint32_t)s * split_bytes;
-        cp_wait_group<UM_RS - 2>();  // this thread's copies of chunk c have landed
-        __syncthreads();             // everyone's have
-        // the products of chunk c - 2 read this split buffer: wait for their commit
-        if (c >= 2 && !bad) bad = !mbar_wait(&bar[s], ((c - 2) >> 1) & 1);
-        if (c % UM_SEG == 0 && g >= 2) {
-            // segment g - 2 ended at chunk (g - 1) UM_SEG - 1 <= c - 2: complete; free its
-            // accumulator for segment g
-            if (__syncthreads_or(bad)) break;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            drain(a, g == 2);
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        }
-        if (!bad) split(raw0 + (uint32_t)(c % UM_RS) * raw_bytes, sbase);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (__syncthreads_or(bad)) break;
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t dacc = tmem + (uint32_t)(a * ntmax);
-            const uint32_t ahi = sbase, alo = sbase + UM_AHALF;
-            const uint32_t bhi = sbase + 2 * UM_AHALF, blo = bhi + (uint32_t)ntmax * (UM_KC * 4);
-#pragma unroll
-            for (int j = 0; j < UM_KC / 8; ++j) {
-                const uint32_t k = (uint32_t)j * 2 * UM_LBO;
-                umma_tf32(dacc, kmajor_desc(ahi + k), kmajor_desc(bhi + k), idesc,
-                          (c % UM_SEG != 0 || j > 0) ? 1u : 0u);
-                umma_tf32(dacc, kmajor_desc(ahi + k), kmajor_desc(blo + k), idesc, 1u);
-                umma_tf32(dacc, kmajor_desc(alo + k), kmajor_desc(bhi + k), idesc, 1u);
-            }
-            umma_commit(&bar[s]);
-        }
-        issue();  // chunk c + UM_RS - 1 into the raw stage chunk c - 1 used
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    // the last commit completes after every product issued before it
-    if (!bad && c > 0) bad = !mbar_wait(&bar[(c - 1) & 1], ((c - 1) >> 1) & 1);
-    bad = __syncthreads_or(bad);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!bad) {
-        // total = FP64 sum of segments 0 .. G-3 + accumulators of segments G-2 and G-1; warps w
-        // and w + 4 take alternate blocks of 8 right-hand sides
-        const int G = (c + UM_SEG - 1) / UM_SEG;
-        auto total8 = [&](int col, double (&v)[8]) {
-            float f[8];
-            tmem_ld8(tlane + (uint32_t)(((G - 1) & 1) * ntmax + col), f);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = f[u];
-            if (G >= 2) {
-                tmem_ld8(tlane + (uint32_t)(((G - 2) & 1) * ntmax + col), f);
-#pragma unroll
-                for (int u = 0; u < 8; ++u) v[u] += f[u];
-            }
-            if (G >= 3) {
-                uint32_t w[16];
-                tmem_ld16(tmaster + 2u * (uint32_t)col, w);
-#pragma unroll
-                for (int u = 0; u < 8; ++u) v[u] += __hiloint2double((int)w[2 * u + 1], (int)w[2 * u]);
             }
         };
-        for (int j8 = half; j8 * 8 < qt; j8 += 2) {
-            double re[8];
-            total8(8 * j8, re);
-            if constexpr (W == 1) {
-                if (row < mt) {
 #pragma unroll
-                    for (int u = 0; u < 8; ++u)
-                        if (8 * j8 + u < qt) out[(int64_t)(q0 + 8 * j8 + u) * nc + m0 + row] = (float)re[u];
+        for (int u = 0; u < 3; ++u)
+            if (u < C) load(ra[u]);
+        for (int c0 = 0; c0 < C; c0 += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int c = c0 + u;
+                if (c >= C || warp_aborted(&abort_s)) break;
+                if (c + 3 < C) load(ra[(u + 3) & 3]);
+                const int s = c % UM_NA;
+                if (c >= UM_NA && !warp_wait(&a_empty[s], ((c / UM_NA) - 1) & 1, limit)) {
+                    abort_s = 1;
+                    break;
                 }
-            } else {
-                double im[8];
-                total8(qt + 8 * j8, im);
-                if (row < mt) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t ta = tl + col_a + (uint32_t)s * a_stage_cols;
+                uint32_t hi[16], lo[16];
+                if constexpr (W == 2) {
+                    // A_re = (ar, -ai), A_im = (ai, ar) per complex k; a = conj(B) for adjoint maps
 #pragma unroll
-                    for (int u = 0; u < 8; ++u)
-                        if (8 * j8 + u < qt)
-                            out[(int64_t)(q0 + 8 * j8 + u) * nc + m0 + row] = T{(float)re[u], (float)im[u]};
+                    for (int j = 0; j < 8; ++j) {
+                        const float ar = ra[u][2 * j], ai = adj ? -ra[u][2 * j + 1] : ra[u][2 * j + 1];
+                        split2(ar, hi[2 * j], lo[2 * j]);
+                        split2(-ai, hi[2 * j + 1], lo[2 * j + 1]);
+                    }
+                    tmem_st16(ta, hi);
+                    tmem_st16(ta + 16, lo);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const float ar = ra[u][2 * j], ai = adj ? -ra[u][2 * j + 1] : ra[u][2 * j + 1];
+                        split2(ai, hi[2 * j], lo[2 * j]);
+                        split2(ar, hi[2 * j + 1], lo[2 * j + 1]);
+                    }
+                    tmem_st16(ta + 32, hi);
+                    tmem_st16(ta + 48, lo);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) split2(ra[u][j], hi[j], lo[j]);
+                    tmem_st16(ta, hi);
+                    tmem_st16(ta + 16, lo);
+                }
+                tmem_wait_st();
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                mbar_arrive(&a_full[s]);
+            }
+            if (warp_aborted(&abort_s)) break;
+        }
+    } else if (warp < 8) {
+        // ---------------- moment warps: B operand into shared memory ----------------
+        const int bt = tid - 128;
+        // this thread's 16-byte pieces (row q, k group kg) of every chunk: pieces bt, bt + 128, ...
+        const int npieces = np * UM_KG;
+        int cp_ = p0, ck = 0;  // copy cursor
+        UmPair<T> cu = um_pair<T>(m, r, t, p0, nc, fwd, nrhs, q0, am);
+        auto issue = [&](int c) {
+            const uint32_t hb = smem0 + (uint32_t)(c % UM_NB) * b_stage_bytes;
+            const int k0 = ck * KQ;
+            for (int pc = bt; pc < npieces; pc += 128) {
+                const int q = pc >> 2, kg = pc & 3;
+                const uint32_t dst = hb + goff(q, kg);
+#pragma unroll
+                for (int e = 0; e < 4 / W; ++e) {
+                    const int k = k0 + kg * (4 / W) + e;
+                    const bool ok = q < qt && k < cu.snc;
+                    const T *src = cu.X;
+                    if (ok) src = cu.X + (int64_t)q * cu.snc + (cu.xmap ? __ldg(cu.xmap + k) : k);
+                    cp_elem<sizeof(T)>(dst + (uint32_t)(e * sizeof(T)), src, ok);
                 }
             }
+            if (++ck == cu.nk) {
+                ck = 0;
+                if (++cp_ < p1) cu = um_pair<T>(m, r, t, cp_, nc, fwd, nrhs, q0, am);
+            }
+        };
+        for (int c = 0; c < UM_LAG && c < C; ++c) {
+            issue(c);
+            cp_commit_group();
+        }
+        for (int c = 0; c < C; ++c) {
+            const int ci = c + UM_LAG;
+            if (ci < C) {
+                // stage ci % UM_NB was last read by the products of chunk ci - UM_NB
+                if (ci >= UM_NB && !mbar_wait(&b_empty[ci % UM_NB], ((ci / UM_NB) - 1) & 1, limit)) abort_s = 1;
+                if (abort_s) break;
+                issue(ci);
+            }
+            cp_commit_group();
+            cp_wait_group<UM_LAG>();  // this thread's copies of chunk c have landed
+            const uint32_t hb = smem0 + (uint32_t)(c % UM_NB) * b_stage_bytes;
+            const uint32_t lb = hb + (uint32_t)np * (UM_KC * 4);
+            for (int pc = bt; pc < npieces; pc += 128) {
+                const uint32_t o = goff(pc >> 2, pc & 3);
+                float v[4];
+                asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                             : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+                             : "r"(hb + o));
+                uint32_t h[4], l[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) split2(v[e], h[e], l[e]);
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(hb + o), "r"(h[0]), "r"(h[1]), "r"(h[2]),
+                             "r"(h[3]));
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(lb + o), "r"(l[0]), "r"(l[1]), "r"(l[2]),
+                             "r"(l[3]));
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(&b_full[c % UM_NB]);
+            if (abort_s) break;
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (warp < 12) {
+        // ---------------- drain warps: FP64 sum of the segments, then the epilogue ----------------
+        const int lq = warp & 3;
+        const int row = 32 * lq + lane;
+        const uint32_t tl = tmem + ((uint32_t)(32 * lq) << 16);
+        bool ok = true;
+        for (int g = 0; g < G; ++g) {
+            const int a = g & 1;
+            if (!warp_wait(&acc_full[a], (g >> 1) & 1, limit)) {
+                abort_s = 1;
+                ok = false;
+                break;
+            }
+            if (warp_aborted(&abort_s)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (uint32_t j = 0; j < acc_cols; j += 8) {
+                uint32_t f[8], w[16];
+                tmem_ld8(tl + (uint32_t)a * acc_cols + j, f);
+                if (g > 0) tmem_ld16(tl + col_master + 2 * j, w);
+                tmem_wait_ld();
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const double prev = g > 0 ? __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]) : 0.0;
+                    const double v = prev + (double)__uint_as_float(f[e]);
+                    w[2 * e] = (uint32_t)__double2loint(v);
+                    w[2 * e + 1] = (uint32_t)__double2hiint(v);
+                }
+                tmem_st16(tl + col_master + 2 * j, w);
+            }
+            tmem_wait_st();
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(&acc_empty[a]);
+        }
+        if (ok && !warp_aborted(&abort_s)) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int j8 = 0; j8 * 8 < qt; ++j8) {
+                uint32_t wr[16], wi[16];
+                tmem_ld16(tl + col_master + 2 * (uint32_t)(8 * j8), wr);
+                if constexpr (W == 2) tmem_ld16(tl + col_master + 2 * (uint32_t)(np + 8 * j8), wi);
+                tmem_wait_ld();
+                if (row < mt) {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        const int q = 8 * j8 + e;
+                        if (q >= qt) break;
+                        const double re = __hiloint2double((int)wr[2 * e + 1], (int)wr[2 * e]);
+                        T *o = out + (int64_t)(q0 + q) * nc + m0 + row;
+                        if constexpr (W == 2) {
+                            const double im = __hiloint2double((int)wi[2 * e + 1], (int)wi[2 * e]);
+                            *o = T{(float)re, (float)im};
+                        } else {
+                            *o = (float)re;
+                        }
+                    }
+                }
+            }
+        }
+    } else if (lane == 0) {
+        // ---------------- MMA thread ----------------
+        const uint32_t idesc = tf32_idesc(UM_M, np);
+        const uint32_t b_hi0 = smem0;
+        int c = 0;
+        for (; c < C; ++c) {
+            const int sa = c % UM_NA, sb = c % UM_NB, g = c / UM_SEG, a = g & 1;
+            if (c % UM_SEG == 0 && g >= 2 && !mbar_wait(&acc_empty[a], ((g >> 1) - 1) & 1, limit)) abort_s = 1;
+            if (!abort_s && !mbar_wait(&a_full[sa], (c / UM_NA) & 1, limit)) abort_s = 1;
+            if (!abort_s && !mbar_wait(&b_full[sb], (c / UM_NB) & 1, limit)) abort_s = 1;
+            if (abort_s) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t dre = tmem + (uint32_t)a * acc_cols;
+            const uint32_t ta = tmem + col_a + (uint32_t)sa * a_stage_cols;
+            const uint32_t bh = b_hi0 + (uint32_t)sb * b_stage_bytes, bl = bh + (uint32_t)np * (UM_KC * 4);
+#pragma unroll
+            for (int j = 0; j < UM_KC / 8; ++j) {
+                const uint64_t dbh = kmajor_desc(bh + (uint32_t)j * 2 * UM_LBO);
+                const uint64_t dbl = kmajor_desc(bl + (uint32_t)j * 2 * UM_LBO);
+                const uint32_t first = (c % UM_SEG != 0 || j > 0) ? 1u : 0u;
+                const uint32_t ah = ta + 8u * j, al = ah + 16u;
+                umma_ts(dre, ah, dbh, idesc, first);
+                umma_ts(dre, ah, dbl, idesc, 1u);
+                umma_ts(dre, al, dbh, idesc, 1u);
+                if constexpr (W == 2) {
+                    const uint32_t dim = dre + (uint32_t)np;
+                    umma_ts(dim, ah + 32u, dbh, idesc, first);
+                    umma_ts(dim, ah + 32u, dbl, idesc, 1u);
+                    umma_ts(dim, al + 32u, dbh, idesc, 1u);
+                }
+            }
+            umma_commit(&a_empty[sa]);
+            umma_commit(&b_empty[sb]);
+            if (c % UM_SEG == UM_SEG - 1 || c == C - 1) umma_commit(&acc_full[a]);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // every role has left its loop
+    if (warp == UM_WARPS - 1 && lane == 0) {
+        // products already issued (all of them, after a wait gave up) may still read the operand
+        // stages and write tensor memory: the issuing thread waits for them, with the full bound,
+        // before the CTA frees its memory
+        umma_commit(&fin);
+        mbar_wait(&fin, 0, UM_SPIN_FINAL);
+    }
     __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
 bool i2o_umma_eligible(bool cplx, int precision, const DMap &m, int nq) {
     // from 4 FP32 columns (2 complex right-hand sides) the MMA tile (padded to N = 16) beats the
-    // FP64 mma.sync tile path (sphere shape at 32,768 points, 2-4 complex RHS: 16.2 vs 20.5 ms per
-    // product); a single right-hand side stays on the FMA tile path (11.9 vs 14.7 ms)
+    // FP64 mma.sync tile path; a single right-hand side stays on the FMA tile path
     return precision == H2B_FP32 && m.coupling_kind == H2B_COUPLING_DENSE && (cplx ? 2 : 1) * nq >= 4;
 }
 
 cudaError_t launch_i2o_umma(bool cplx, const DMap &m, const DSide &recv, const DSide &src, const int *nodes,
                             int nnodes, const FarArgs &fa, int maxcoef, cudaStream_t st) {
     if (nnodes == 0) return cudaSuccess;
-    const int W = cplx ? 2 : 1;
     const int nq = m.ncomp * fa.nrhs;
-    // right-hand sides per tile: MMA N = W * qt <= 64, tiles of equal width
-    const int ntiles = (W * nq + UM_NT_MAX - 1) / UM_NT_MAX;
+    const int ntmax = cplx ? UM_NT_MAX_CPLX : UM_NT_MAX_REAL;
+    // right-hand sides per tile: at most ntmax, tiles of equal width
+    const int ntiles = (nq + ntmax - 1) / ntmax;
     const int qt_max = (nq + ntiles - 1) / ntiles;
-    const int ntmax = ((W * qt_max + 15) / 16) * 16;
-    const int lbmax = cplx ? ((qt_max + 7) / 8) * 8 : ntmax;
-    // two split buffers (A and B, TF32 hi and lo) and UM_RS raw stages
-    const size_t smem = 2 * (2 * (size_t)UM_AHALF + 2 * (size_t)ntmax * (UM_KC * 4)) +
-                        (size_t)UM_RS * (UM_RAWA + (size_t)lbmax * UM_RAWROW);
+    const int np = ((qt_max + 15) / 16) * 16;
+    const size_t smem = (size_t)UM_NB * 2 * np * UM_KC * 4;  // moment stages (hi and lo)
     const dim3 grid(nnodes, (maxcoef + UM_M - 1) / UM_M, ntiles);
     auto go = [&](auto kern, auto *am, auto *dm) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -574,6 +608,15 @@ cudaError_t launch_i2o_umma(bool cplx, const DMap &m, const DSide &recv, const D
 
 cudaError_t read_umma_timeouts(unsigned *count) {
     return cudaMemcpyFromSymbol(count, g_umma_timeouts, sizeof(unsigned));
+}
+
+cudaError_t copy_umma_timeouts_async(unsigned *host, cudaStream_t st) {
+    return cudaMemcpyFromSymbolAsync(host, g_umma_timeouts, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, st);
+}
+
+cudaError_t set_umma_wait_limit(unsigned limit) {
+    const unsigned v = limit ? limit : UM_SPIN;
+    return cudaMemcpyToSymbol(g_umma_wait_limit, &v, sizeof(unsigned));
 }
 
 }  // namespace h2b

@@ -223,6 +223,13 @@ const char *h2b_last_error(void);
  * No counterpart in the reference: its CPU map has no device-side waits. */
 h2b_status h2b_tensor_wait_timeouts(int32_t device, uint32_t *count);
 
+/* Bound of every mbarrier wait of the tensor-core kernels on `device`, in try_wait attempts; 0
+ * restores the default (2^22). A low bound makes the waits give up, which is how tests exercise
+ * the timeout path without faulting or hanging anything: the kernels then stop, wait for the
+ * products they issued, free their tensor memory and return, and h2b_matvec_host reports
+ * H2B_ERR_CUDA. Waits for the device's queued work. No counterpart in the reference. */
+h2b_status h2b_set_tensor_wait_limit(int32_t device, uint32_t limit);
+
 /* Validate `desc`, copy it to `device` and build the read-only core: the CUDA equivalent of
  * building an AbstractH2Core (src/maps/core.jl:17-33). The caller keeps its host arrays. */
 h2b_status h2b_core_create(const h2b_map_desc *desc, int32_t device, h2b_core **out);
@@ -260,7 +267,9 @@ h2b_status h2b_matvec(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void 
                       void *stream);
 
 /* Same product on HOST arrays: copies x in, multiplies, copies y out and synchronizes the
- * stream before returning. This is the call a host-language binding makes for mul!(y, A, x). */
+ * stream before returning. This is the call a host-language binding makes for mul!(y, A, x).
+ * Returns H2B_ERR_CUDA when a bounded tensor-core wait on the device gave up while the product ran
+ * (its output is then incomplete; h2b_tensor_wait_timeouts counts such waits). */
 h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
                            int64_t ldx, void *y, int64_t ldy, const double *alpha,
                            const double *beta, void *stream);
@@ -275,6 +284,35 @@ h2b_status h2b_matvec_host(h2b_workspace *ws, int32_t mode, int32_t nrhs, const 
 h2b_status h2b_matvec_host_async(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x,
                                  int64_t ldx, void *y, int64_t ldy, const double *alpha,
                                  const double *beta, void *stream);
+
+/* Passes of a product, for h2b_profile_matvec. The far passes follow farmul!
+ * (src/farinteractions/farmul.jl:47-70): leaf aggregation, one upward transfer per level, the
+ * Toeplitz forward transforms, I2O, the inverse transforms, one downward transfer per level and the
+ * leaf disaggregation. */
+#define H2B_PASS_NEAR 0
+#define H2B_PASS_LEAF_AGGREGATE 1
+#define H2B_PASS_AGGREGATE 2        /* upward transfers into the nodes of one level */
+#define H2B_PASS_MODULATE_IN 3
+#define H2B_PASS_I2O 4
+#define H2B_PASS_MODULATE_OUT 5
+#define H2B_PASS_DISAGGREGATE 6     /* downward transfers into the nodes of one level */
+#define H2B_PASS_LEAF_DISAGGREGATE 7
+
+typedef struct h2b_pass_time {
+    int32_t pass;         /* H2B_PASS_* */
+    int32_t level;        /* level of the nodes the launch writes; 0 when it spans every level */
+    double milliseconds;  /* device time of the launch (CUDA events on the caller's stream) */
+} h2b_pass_time;
+
+/* The product of h2b_matvec (same arguments and result) with every pass timed on the device:
+ * Diagnostics.profilemul / timedmul! (src/diagnostics/timing.jl:122-160), whose records name an
+ * operation, its phase and level. The near pass and the far passes run one after another on
+ * `stream` (h2b_matvec overlaps them), an event is recorded after each launch, and the call
+ * synchronizes the stream before it returns. Writes up to `capacity` records in launch order and
+ * the number of passes in *count. Not allowed inside a stream capture (H2B_ERR_INVALID). */
+h2b_status h2b_profile_matvec(h2b_workspace *ws, int32_t mode, int32_t nrhs, const void *x, int64_t ldx,
+                              void *y, int64_t ldy, const double *alpha, const double *beta, void *stream,
+                              h2b_pass_time *records, int32_t capacity, int32_t *count);
 
 /* Far part only: farmul! (src/farinteractions/farmul.jl:8-70). With alpha = beta = NULL y is
  * zero-filled first (3-argument form); otherwise only leaves that receive a far contribution

@@ -2,7 +2,7 @@
 
 Tolerances: the FP64 form must match the oracle to a relative L2 error of 1e-12 (the bar of
 docs/src/implementing/example.md:205-222); the FP32 far-field form must match the FP64 oracle to
-1e-5 (its near field and final summation stay FP64).
+1e-6, the reduced-precision bar of the served form (its near field and final summation stay FP64).
 """
 
 import os
@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 DEV = "cuda:0"
 TOL64 = 1e-12
-TOL32 = 1e-5
+TOL32 = 1e-6
 
 
 def rel(a, b):

@@ -62,6 +62,7 @@ def _core(cores, name):
 ])
 def test_tensor_i2o_matches_fp64(cores, name, nrhs):
     core = _core(cores, name)
+    timeouts = _abi.tensor_wait_timeouts(0)
     ws64 = h2.H2Workspace(core, max_nrhs=nrhs)
     ws32 = h2.H2Workspace(_fp32(core), max_nrhs=nrhs)
     for mode, op in ORIENT:
@@ -74,13 +75,14 @@ def test_tensor_i2o_matches_fp64(cores, name, nrhs):
         got_far = run(h2.farmul_, op(ws32), x)
         err_far = rel(got_far, want_far)
         assert err_far < TOL32, (name, nrhs, mode, err_far)
-    assert _abi.tensor_wait_timeouts(0) == 0
+    assert _abi.tensor_wait_timeouts(0) == timeouts
 
 
 def test_tensor_i2o_sphere_against_oracle(cores):
     """216 coefficients (two row tiles), 32 complex right-hand sides (one 64-column tile),
     symmetry-reduced couplings: forward and adjoint against the FP64 oracle."""
     core = _core(cores, "sphere-cheb6-helmholtz-sym")
+    timeouts = _abi.tensor_wait_timeouts(0)
     ws32 = h2.H2Workspace(_fp32(core), max_nrhs=32)
     desc = h2.flatten(core)
     for mode, op in (ORIENT[0], ORIENT[2]):
@@ -89,7 +91,7 @@ def test_tensor_i2o_sphere_against_oracle(cores):
         assert rel(run(h2.mul_, op(ws32), x), want) < BAR, mode
         want_far = oracle.farmul(core, x, mode, desc=desc)
         assert rel(run(h2.farmul_, op(ws32), x), want_far) < TOL32, mode
-    assert _abi.tensor_wait_timeouts(0) == 0
+    assert _abi.tensor_wait_timeouts(0) == timeouts
 
 
 def test_tensor_i2o_repeatable(cores):
