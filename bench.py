@@ -588,7 +588,7 @@ def core_with_host_near(core, near_host):
     return c
 
 
-def sphere_core(n, device, precision="fp64"):
+def sphere_core(n, device, precision="fp64", transfers="dense"):
     """The sphere configuration's map at `n` points: Fibonacci sphere (radius 0.45 in the unit
     cube) with jitter 0.1 x spacing, leaves <= 128 points, Helmholtz k = 8 pi x 0.45 (the unit
     sphere's electrical size), Chebyshev p = 6, symmetry-reduced couplings, near blocks assembled
@@ -604,7 +604,7 @@ def sphere_core(n, device, precision="fp64"):
     tree = trees.build_tree(0.5 + 0.45 * p, maxvalues=128, root_center=[0.5] * 3, root_halfsize=0.5)
     k = 8 * np.pi * 0.45
     core = methods.interpolation_core(tree, methods.helmholtz(k), 6, near="none", symmetry=True,
-                                      precision=precision)
+                                      precision=precision, transfers=transfers)
     assembly.near_blocks_device(core, "helmholtz", wavenumber=k, device=device)
     return h2, core
 
@@ -676,7 +676,7 @@ def sphere_arm(args):
     import torch
 
     device = "cuda:0"
-    h2, core = sphere_core(args.n, device)
+    h2, core = sphere_core(args.n, device, transfers=args.transfers)
     n = core.trial.npoints
     stream = torch.cuda.current_stream(device)
     x = torch.randn((32, n), dtype=torch.complex128, device=device).t()
@@ -732,6 +732,8 @@ def main():
                     help="time the batched-uneven configuration's shape (eager vs one graph replay per pass)")
     ap.add_argument("--maps", type=int, default=96, help="maps of the batched mode")
     ap.add_argument("--nmax", type=int, default=16384, help="largest point count of the batched mode")
+    ap.add_argument("--transfers", default="dense", choices=["dense", "separable"],
+                    help="level transfers of the sphere mode's map")
     ap.add_argument("--sphere", action="store_true",
                     help="time the sphere configuration's shape at --n points instead (dense far field)")
     args = ap.parse_args()

@@ -719,12 +719,20 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
             uptr[g + 1] = (int)ulist.size();
         }
         if (ulist.empty()) ulist.push_back(make_int4(0, 0, 0, 0));
+        std::vector<int2> slabs;
+        for (size_t g = 0; g < leaf.size(); ++g)
+            for (int r0 = 0; r0 < nv(out, leaf[g]); r0 += 32) slabs.push_back(make_int2((int)g, r0 / 32));
+        op.nslabs = (int)slabs.size();
+        if (slabs.empty()) slabs.push_back(make_int2(0, 0));
         int *pp;
         int4 *pu;
+        int2 *ps;
         CUDA_TRY(c->upload(&pp, uptr.data(), uptr.size()));
         CUDA_TRY(c->upload(&pu, ulist.data(), ulist.size()));
+        CUDA_TRY(c->upload(&ps, slabs.data(), slabs.size()));
         op.unit_ptr = pp;
         op.unit = pu;
+        op.slab = ps;
         return H2B_OK;
     };
     int *p;
@@ -1150,6 +1158,9 @@ h2b_status h2b_workspace_create(h2b_core *core, int32_t max_nrhs, h2b_workspace 
     if (e == cudaSuccess) e = al(&ws->ybuf, ndof * vsz);
     if (e == cudaSuccess && !cplx && max_nrhs >= 8)
         e = al(&ws->xnear, (size_t)std::max(core->test.ndofs, core->trial.ndofs) * 16 * sizeof(double));
+    if (e == cudaSuccess && cplx && max_nrhs >= 8 && core->dnear.kind == H2B_NEAR_STORED)
+        e = al(&ws->xnear, (size_t)std::max(core->test.ndofs, core->trial.ndofs) * near_rhs_block(max_nrhs) * 2 *
+                               sizeof(double));
     // the far passes (a chain of dependent launches, the critical path) run on this stream at the
     // device's greatest priority, so their blocks are scheduled ahead of the near field's, which
     // fills the SMs around them

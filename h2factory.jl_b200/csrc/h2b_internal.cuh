@@ -120,6 +120,10 @@ struct NearOp {
     const int *unit_ptr = nullptr;  // [ngroups+1]
     const int4 *unit = nullptr;
     const void *data = nullptr;     // V
+    // (group, 32-row slab) pairs covering every output row: the work items of the complex
+    // tensor-core near kernel, one warp each
+    int nslabs = 0;
+    const int2 *slab = nullptr;
 };
 
 struct DNear {
@@ -199,6 +203,8 @@ cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &test, 
                         int nrhs, const void *x, int64_t ldx, void *y, int64_t ldy, cdouble alpha,
                         cdouble beta, void *xp, cudaStream_t st);
 int64_t near_padded_ld(bool cplx, int n);
+// right-hand sides per pass of the complex tensor-core near kernel for a block of `nrhs`
+int near_rhs_block(int nrhs);
 cudaError_t launch_near_repack(bool cplx, const void *src, const int64_t *src_off, const int *blk_row,
                                const int *blk_col, const DSide &rows, const DSide &cols, void *dst,
                                const int64_t *dst_off, int nblocks, bool transpose, cudaStream_t st);

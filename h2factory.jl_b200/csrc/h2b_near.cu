@@ -374,6 +374,151 @@ cudaError_t launch_rows_mma(const NearOp &op, const DSide &outs, const DSide &in
 
 
 
+// Complex near blocks, 8 or more right-hand sides, on the FP64 tensor cores. One warp (one CTA)
+// per (output leaf, 32-row slab) work item (NearOp::slab): the warp streams the slab's rows of
+// every block of the leaf through a private CST-stage cp.async ring (CCOLS columns and their
+// gathered x rows per stage, zero-filled past the block) and keeps all R right-hand sides of its
+// 32 rows in registers, so no partial rows are exchanged between warps and the block scheduler
+// balances the items. A complex product runs as a real one without rearranging the stored block:
+// its column k read as the two real columns (re, im) is the A operand along k' = 2k, 2k + 1, and
+// with B rows [xr, xi] and [-xi, xr] (adjoint: [xi, -xr]) the real output columns are [Re y | Im y]:
+//   Re y = sum_k ar xr - ai xi,  Im y = sum_k ar xi + ai xr.
+// Fragment row g of row tile t is slab row 4g + t (m8n8k4: A[lane/4][lane%4], B[lane%4][lane/4]).
+constexpr int CST = 3;     // ring stages per warp
+constexpr int CCOLS = 4;   // complex columns per stage: two k steps
+constexpr int CSA = 33;    // slab column stride in complex elements (32 rows + 1 of padding)
+
+template <int R>
+__global__ void __launch_bounds__(32, 16)
+near_slab_mma_c_kernel(NearOp op, DSide outs, int r0, int rc, const cdouble *__restrict__ xp,
+                       cdouble *__restrict__ y, int64_t ldy, cdouble alpha, cdouble beta, bool beta_zero,
+                       bool cjg) {
+    constexpr int NU = R / 8;                        // n tiles per block of R real columns
+    constexpr int XS = R + 1;                        // x row stride (complex)
+    constexpr int SS = CCOLS * CSA + CCOLS * XS;     // complex elements per stage
+    __shared__ __align__(16) cdouble ring[CST * SS];
+    const int2 item = op.slab[blockIdx.x];
+    const int g = item.x, rows0 = 32 * item.y;
+    const int leaf = op.grp_leaf[g];
+    const int o0 = outs.value_ptr[leaf], nr = outs.value_ptr[leaf + 1] - o0;
+    const int nrows = min(32, nr - rows0);
+    const int u0 = op.unit_ptr[g], u1 = op.unit_ptr[g + 1];
+    const int lane = threadIdx.x, g4 = lane >> 2, t4 = lane & 3;
+    const cdouble *D = static_cast<const cdouble *>(op.data);
+    // producer cursor: unit pu, its entry ue, first column pj of the next stage
+    int pu = u0, pj = 0;
+    int4 ue = pu < u1 ? op.unit[pu] : make_int4(0, 0, 0, 0);
+    auto issue = [&](int slot) -> int {  // one commit group per call; 1 if it holds a stage
+        int got = 0;
+        if (pu < u1) {
+            const int c0 = ue.x, nc = ue.y;
+            const cdouble *B = D + (((int64_t)ue.w << 32) | (uint32_t)ue.z) + rows0;
+            cdouble *sa = ring + slot * SS, *sx = sa + CCOLS * CSA;
+#pragma unroll
+            for (int col = 0; col < CCOLS; ++col) {
+                const bool ok = pj + col < nc && lane < nrows;
+                cp16(sa + col * CSA + lane, ok ? B + (int64_t)(pj + col) * nr + lane : B, ok);
+            }
+#pragma unroll
+            for (int c = lane; c < CCOLS * R; c += 32) {
+                const int col = c / R, q = c % R;
+                const bool ok = pj + col < nc;
+                cp16(sx + col * XS + q, ok ? xp + (int64_t)(c0 + pj + col) * R + q : xp, ok);
+            }
+            got = 1;
+            pj += CCOLS;
+            if (pj >= nc) {
+                pj = 0;
+                if (++pu < u1) ue = op.unit[pu];
+            }
+        }
+        cp_commit();
+        return got;
+    };
+    double acc[4][2 * NU][2];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int u = 0; u < 2 * NU; ++u) acc[t][u][0] = acc[t][u][1] = 0.0;
+    int nst = 0;
+#pragma unroll
+    for (int s2 = 0; s2 < CST - 1; ++s2) nst += issue(s2);
+    int slot = 0;
+    const int part = t4 & 1;
+    for (int st = 0; st < nst; ++st) {
+        nst += issue((slot + CST - 1) % CST);
+        cp_wait<CST - 1>();
+        __syncwarp();
+        const double *sa = reinterpret_cast<const double *>(ring + slot * SS);
+        const cdouble *sx = ring + slot * SS + CCOLS * CSA;
+#pragma unroll
+        for (int kk = 0; kk < CCOLS / 2; ++kk) {
+            const int col = 2 * kk + (t4 >> 1);
+            double a[4], b[2 * NU];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) a[t] = sa[2 * (col * CSA + 4 * g4 + t) + part];
+#pragma unroll
+            for (int u = 0; u < NU; ++u) {
+                const double2 xv = *reinterpret_cast<const double2 *>(sx + col * XS + 8 * u + g4);
+                if (part == 0) {
+                    b[u] = xv.x;
+                    b[NU + u] = xv.y;
+                } else {
+                    b[u] = cjg ? xv.y : -xv.y;
+                    b[NU + u] = cjg ? -xv.x : xv.x;
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+#pragma unroll
+                for (int u = 0; u < 2 * NU; ++u) dmma(acc[t][u], a[t], b[u]);
+        }
+        __syncwarp();  // the slot is read; the next issue may refill it
+        slot = slot + 1 == CST ? 0 : slot + 1;
+    }
+    cp_wait<0>();
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int row = 4 * g4 + t;
+        if (row >= nrows) continue;
+        const int64_t dof = outs.value[o0 + rows0 + row];
+#pragma unroll
+        for (int u = 0; u < NU; ++u)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int q = 8 * u + 2 * t4 + i;
+                if (q >= rc) continue;
+                cdouble *o = &y[(int64_t)(r0 + q) * ldy + dof];
+                const cdouble v = alpha * cdouble{acc[t][u][i], acc[t][NU + u][i]};
+                *o = beta_zero ? v : v + beta * *o;
+            }
+    }
+}
+
+// complex x rows gathered in leaf order: xp[pos * R + q] = x[(r0 + q) * ldx + value[pos]]
+template <int R>
+__global__ void near_gather_c_kernel(const int *__restrict__ value, int nvals, int r0, int rc,
+                                     const cdouble *__restrict__ x, int64_t ldx, cdouble *__restrict__ xp) {
+    const int64_t total = (int64_t)nvals * R;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int pos = (int)(e / R), q = (int)(e % R);
+        xp[e] = q < rc ? x[(int64_t)(r0 + q) * ldx + value[pos]] : cdouble{0.0, 0.0};
+    }
+}
+
+template <int R>
+cudaError_t launch_slab_mma_c(const NearOp &op, const DSide &outs, const DSide &ins, bool cjg, int r0, int rc,
+                              const cdouble *x, int64_t ldx, cdouble *xp, cdouble *y, int64_t ldy, cdouble alpha,
+                              cdouble beta, bool bz, cudaStream_t st) {
+    const int nvals = ins.nvalues;
+    near_gather_c_kernel<R><<<std::max(1, std::min(148 * 8, (int)(((int64_t)nvals * R + 255) / 256))), 256, 0, st>>>(
+        ins.value, nvals, r0, rc, x, ldx, xp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || op.nslabs == 0) return e;
+    near_slab_mma_c_kernel<R><<<op.nslabs, 32, 0, st>>>(op, outs, r0, rc, xp, y, ldy, alpha, beta, bz, cjg);
+    return cudaGetLastError();
+}
+
 // Matrix-free near field ---------------------------------------------------------------------
 // The point kernels of H2B_NEAR_LAPLACE / H2B_NEAR_HELMHOLTZ: the entry of (output dof i, input
 // dof j) from their squared distance; 0 for coincident points (the self term).
@@ -608,6 +753,22 @@ cudaError_t near_apply_t(const NearOp &op, const DSide &outs, const DSide &ins, 
                          const V *x, int64_t ldx, V *y, int64_t ldy, V alpha, V beta, bool bz,
                          double *xp, cudaStream_t st) {
     if (op.ngroups == 0) return cudaSuccess;
+    if constexpr (std::is_same<V, cdouble>::value) {
+        // complex blocks, 8 or more right-hand sides (workspaces that size carry the gather
+        // buffer): FP64 tensor cores, 16 right-hand sides per pass over the blocks (32 would hold
+        // 64 FP64 accumulators per lane and spill)
+        const int rb = near_rhs_block(nrhs);
+        int r0 = 0;
+        for (; xp && r0 < nrhs && nrhs - r0 >= 8; r0 += rb) {
+            const int rc = std::min(rb, nrhs - r0);
+            cudaError_t e = launch_slab_mma_c<16>(op, outs, ins, cjg, r0, rc, x, ldx, (cdouble *)xp, y, ldy, alpha,
+                                                  beta, bz, st);
+            if (e != cudaSuccess) return e;
+        }
+        x += r0 * ldx;
+        y += r0 * ldy;
+        nrhs -= r0;
+    }
     for (int r0 = 0; r0 < nrhs; r0 += 16) {
         const int rc = std::min(16, nrhs - r0);
         cudaError_t e;
@@ -638,6 +799,8 @@ cudaError_t near_apply_t(const NearOp &op, const DSide &outs, const DSide &ins, 
 }  // namespace
 
 int64_t near_padded_ld(bool cplx, int n) { return cplx ? n : n + (n & 1); }
+
+int near_rhs_block(int) { return 16; }
 
 cudaError_t launch_near_repack(bool cplx, const void *src, const int64_t *src_off, const int *blk_row,
                                const int *blk_col, const DSide &rows, const DSide &cols, void *dst,
@@ -695,7 +858,7 @@ cudaError_t launch_near(bool cplx, int mode, const DNear &n, const DSide &test, 
     if (cplx)
         return near_apply_t<cdouble>(op, outs, ins, cjg, nrhs, static_cast<const cdouble *>(x), ldx,
                                      static_cast<cdouble *>(y), ldy, alpha, beta,
-                                     beta.x == 0.0 && beta.y == 0.0, nullptr, st);
+                                     beta.x == 0.0 && beta.y == 0.0, static_cast<double *>(xp), st);
     return near_apply_t<double>(op, outs, ins, false, nrhs, static_cast<const double *>(x), ldx,
                                 static_cast<double *>(y), ldy, alpha.x, beta.x, beta.x == 0.0,
                                 static_cast<double *>(xp), st);

@@ -13,13 +13,14 @@
 //     a register ring (the couplings are L2-resident), split chunk c into TF32 high parts and
 //     rounded remainders and write them into a tensor-memory stage with tcgen05.st. The MMAs take
 //     this operand (A) straight from tensor memory, so it never passes through shared memory;
-//   * moment warps (4-7): cp.async each chunk's source moments (B) into a shared-memory stage of
+//   * moment warps (4-6): cp.async each chunk's source moments (B) into a shared-memory stage of
 //     an 8-deep ring in the canonical no-swizzle K-major layout, then split their own elements in
 //     place into TF32 high parts plus a remainder buffer;
-//   * one MMA thread (warp 12): per 8-wide k step the products hi*hi + hi*lo + lo*hi (the lo*lo
+//   * one MMA thread (warp 11): per 8-wide k step the products hi*hi + hi*lo + lo*hi (the lo*lo
 //     term is below FP32 rounding) into an FP32 accumulator in tensor memory; commits release the
 //     operand stages;
-//   * drain warps (8-11): the tensor cores round each accumulation toward zero, so one FP32
+//   * drain warps (7-10, one per tensor-memory lane quarter): the tensor cores round each
+//     accumulation toward zero, so one FP32
 //     accumulator over a whole interaction list loses ~1e-4; accumulators live for 8 chunks only,
 //     two alternate, and each finished one is added into an FP64 sum in tensor memory, which the
 //     epilogue rounds once into the FP32 moments.
@@ -49,7 +50,11 @@ constexpr int UM_NA = 4;          // coupling stages in tensor memory
 constexpr int UM_NB = 8;          // moment stages in shared memory
 constexpr int UM_LAG = UM_NB - 2; // moment copies issued this many chunks ahead of the split
 constexpr int UM_SEG = 8;         // chunks per accumulation segment
-constexpr int UM_WARPS = 13;      // 4 coupling, 4 moment, 4 drain, 1 MMA
+// 4 coupling, 3 moment, 4 drain, 1 MMA: twelve warps place three on each SM sub-partition, whose
+// 16K registers then allow up to 170 per thread (a thirteenth warp would cap them at 128)
+constexpr int UM_WARPS = 12;
+constexpr int UM_BW = 3;           // moment warps
+constexpr int UM_BT = UM_BW * 32;  // moment threads
 constexpr int UM_THREADS = UM_WARPS * 32;
 constexpr int UM_NT_MAX_REAL = 64;    // MMA N (right-hand sides) per tile, real maps
 constexpr int UM_NT_MAX_CPLX = 32;    // complex maps (two accumulators: Re and Im)
@@ -240,7 +245,7 @@ __device__ __forceinline__ float2 ldg2(const cfloat *p) { return __ldg(reinterpr
 }  // namespace
 
 template <class T>
-__global__ void __maxnreg__(152)
+__global__ void __maxnreg__(168)
 i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mode, int nrhs, int qt_max,
                 const T *__restrict__ am, T *__restrict__ dm) {
     constexpr int W = UmScalar<T>::W;
@@ -291,7 +296,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             mbar_init(&a_empty[s], 1);
         }
         for (int s = 0; s < UM_NB; ++s) {
-            mbar_init(&b_full[s], 128);
+            mbar_init(&b_full[s], UM_BT);
             mbar_init(&b_empty[s], 1);
         }
         for (int a = 0; a < 2; ++a) {
@@ -405,17 +410,17 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             }
             if (warp_aborted(&abort_s)) break;
         }
-    } else if (warp < 8) {
+    } else if (warp < 4 + UM_BW) {
         // ---------------- moment warps: B operand into shared memory ----------------
         const int bt = tid - 128;
-        // this thread's 16-byte pieces (row q, k group kg) of every chunk: pieces bt, bt + 128, ...
+        // this thread's 16-byte pieces (row q, k group kg) of every chunk: pieces bt, bt + UM_BT, ...
         const int npieces = np * UM_KG;
         int cp_ = p0, ck = 0;  // copy cursor
         UmPair<T> cu = um_pair<T>(m, r, t, p0, nc, fwd, nrhs, q0, am);
         auto issue = [&](int c) {
             const uint32_t hb = smem0 + (uint32_t)(c % UM_NB) * b_stage_bytes;
             const int k0 = ck * KQ;
-            for (int pc = bt; pc < npieces; pc += 128) {
+            for (int pc = bt; pc < npieces; pc += UM_BT) {
                 const int q = pc >> 2, kg = pc & 3;
                 const uint32_t dst = hb + goff(q, kg);
 #pragma unroll
@@ -448,7 +453,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             cp_wait_group<UM_LAG>();  // this thread's copies of chunk c have landed
             const uint32_t hb = smem0 + (uint32_t)(c % UM_NB) * b_stage_bytes;
             const uint32_t lb = hb + (uint32_t)np * (UM_KC * 4);
-            for (int pc = bt; pc < npieces; pc += 128) {
+            for (int pc = bt; pc < npieces; pc += UM_BT) {
                 const uint32_t o = goff(pc >> 2, pc & 3);
                 float v[4];
                 asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
@@ -467,7 +472,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             if (abort_s) break;
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
-    } else if (warp < 12) {
+    } else if (warp < UM_WARPS - 1) {
         // ---------------- drain warps: FP64 sum of the segments, then the epilogue ----------------
         const int lq = warp & 3;
         const int row = 32 * lq + lane;

@@ -215,10 +215,16 @@ static void SFX(transfer)(const h2b_map_desc *d, const h2b_side_desc *s, int chi
  * ifft with e^{+2πi jk/n} and 1/n per axis (toeplitzmul.jl:290-315). Plain DFT per axis.
  * ------------------------------------------------------------------------------------------- */
 static void SFX(dft_axes)(double _Complex *a, const int *ts, int inverse) {
-    double _Complex line[64], outl[64];
+    double _Complex line[64], outl[64], tw[64];
     for (int ax = 0; ax < 3; ++ax) {
         const int n = ts[ax];
         if (n == 1) continue;
+        /* the twiddle of (j, k) depends on j k mod n only: one table per axis (an FFTW plan's role,
+           ext/H2Toeplitz/toeplitzi2ocollection.jl:34-58), the same values the direct sum used */
+        for (int m = 0; m < n; ++m) {
+            const double ang = (inverse ? 2.0 : -2.0) * M_PI * (double)m / n;
+            tw[m] = cos(ang) + I * sin(ang);
+        }
         const int64_t stride = ax == 0 ? 1 : (ax == 1 ? ts[0] : (int64_t)ts[0] * ts[1]);
         const int64_t total = (int64_t)ts[0] * ts[1] * ts[2];
         for (int64_t base = 0; base < total; ++base) {
@@ -227,10 +233,7 @@ static void SFX(dft_axes)(double _Complex *a, const int *ts, int inverse) {
             for (int k = 0; k < n; ++k) line[k] = a[base + k * stride];
             for (int k = 0; k < n; ++k) {
                 double _Complex acc = 0;
-                for (int j = 0; j < n; ++j) {
-                    const double ang = (inverse ? 2.0 : -2.0) * M_PI * (double)((int64_t)j * k % n) / n;
-                    acc += line[j] * (cos(ang) + I * sin(ang));
-                }
+                for (int j = 0; j < n; ++j) acc += line[j] * tw[(int64_t)j * k % n];
                 outl[k] = inverse ? acc / n : acc;
             }
             for (int k = 0; k < n; ++k) a[base + k * stride] = outl[k];

@@ -115,9 +115,12 @@ def test_noalloc_matches_workspace_farmul_twice(name):
 
 def test_noalloc_thirteen_rhs_toeplitz():
     """13 right-hand sides: the multi-RHS kernels (FP64 tensor-core sibling I2O, a partial 16-wide
-    block) take their arenas from the scratch too."""
-    core, tol = next((c, t) for n, c, t in _maps() if n == "toeplitz-laplace")
-    _check_twice(core, tol, 13, seed=11)
+    block) take their arenas from the scratch too (a depth-3 Toeplitz map, whose arenas for 13
+    right-hand sides fit the scratch)."""
+    rng = np.random.default_rng(4)
+    t = build_tree(rng.random((1500, 3)), depth=3, root_center=[0.5] * 3, root_halfsize=0.5)
+    core = methods.interpolation_core(t, methods.laplace, 3, nodes="equispaced", couplings="toeplitz")
+    _check_twice(core, TOL64, 13, seed=11)
 
 
 def test_noalloc_scratch_almost_full():
