@@ -1,26 +1,41 @@
-"""Benchmark of the B200 H2 matvec on the Toeplitz far-field workload.
+"""Benchmark of the B200 H2 matvec.
 
-Workload (synthetic, seeded): Laplace kernel 1/(4 pi |x-y|), N = 262144 points uniform in the unit
-cube, uniform octree of depth 5 (4096 leaves, ~64 points per leaf), equispaced interpolation p = 4
-per axis with Toeplitz M2L (FFT on (2p-1)^3 = 7^3 padded grids), dense FP64 near blocks of adjacent
-leaves (97,336 blocks, ~399 M entries). One step = one matvec on one right-hand-side block,
-alternating forward and transpose. Two forms are timed: plain (FP64 everywhere, one right-hand
-side per matvec) and served (FP32 far field, FP64 near field and final sum, R = 16 right-hand sides
-coalesced per matvec); `value` is the served form's throughput, `plain` the plain form's. The near
-blocks (3.2 GB) exceed L2 (126 MB), so no L2 flush is needed between steps.
+Default workload (the largest single-GPU configuration of the benchmark set; synthetic, seeded):
+Helmholtz kernel exp(ik|x-y|)/(4 pi |x-y|) with k = 8 pi x 0.45 (eight wavelengths across the
+sphere), N = 1,048,576 points quasi-uniform on a sphere of radius 0.45 (Fibonacci lattice with
+seeded jitter of 0.1 spacing), octree split while a box holds more than 128 points, Chebyshev
+interpolation p = 6 (216 coefficients per box) with separable level transfers and
+symmetry-reduced dense M2L couplings, dense complex near blocks of adjacent leaves (1.11 G
+entries, 17.8 GB, assembled on the device). One step = one matvec on a block of 32 complex
+right-hand sides, alternating forward and adjoint.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--nrhs R]
+Two forms of the same map are timed:
+  * plain:  ComplexF64 everywhere, one request at a time;
+  * served: ComplexF32 far field (moments, transfers, couplings; dense M2L on the tcgen05 tensor
+            cores with a three-term TF32 split), FP64 near field and near + far sum, `--inflight`
+            requests in flight on their own workspaces and streams, as the serving loop runs them.
+`value` is the served form's right-hand sides per second (device time of all requests, max over
+ranks), `plain` the plain form's. `e2e` is the served form through the host-buffer C-ABI call
+(h2b_matvec_host_async: each request copies its x block in and its y block out, pinned memory,
+copies inside the host-clocked region). The near blocks (17.8 GB) exceed L2, so no flush is needed.
+A second leg times the Toeplitz configuration (Laplace, N = 262,144 uniform in the unit cube,
+depth-5 octree, equispaced p = 4 with FFT'd M2L) in the same two forms (`toeplitz` in the line).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload sphere|toeplitz]
 
 Rank 0 prints one JSON line. With N > 1 every rank runs an independent replica of the map (the
 single-map product does not shard), timing is the max over ranks, and `value` is the total
-right-hand sides of all ranks per second.
+right-hand sides of all ranks per second. `--impl reference` times the CPU port of the reference
+algorithm (oracle/) on the same workload.
 """
 
 from __future__ import annotations
 
 import argparse
+import copy
 import importlib.util
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -33,7 +48,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "h2factory.jl_b200")
 METRIC = "H2 matvec RHS/s + p50/p99 latency at <=1e-6 rel err vs FP64; served vs plain"
-WORKLOAD = "toeplitz-laplace-N262144-depth5-p4"
+SPHERE_K = 8 * np.pi * 0.45
 
 
 def _package():
@@ -48,12 +63,14 @@ def _package():
 
 
 def peaks():
+    """(HBM GB/s, dense bf16 TFLOP/s burst, kind): the measured copy bandwidth and cuBLAS bf16 rate
+    of this pool's B200s, else the recorded fallback."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
         with open(path) as f:
             p = json.load(f)
-        return float(p["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
 
 
 def traffic_table():
@@ -66,48 +83,6 @@ def traffic_table():
             if len(parts) >= 3 and not line.startswith("#"):
                 out[(parts[0], parts[1])] = float(parts[2])
     return out
-
-
-# ---------------------------------------------------------------------------------------------
-# workload
-# ---------------------------------------------------------------------------------------------
-def build_core(n=262144, depth=5, p=4, seed=0, device="cuda:0", precision="fp64"):
-    h2 = _package()
-    from h2factory_b200 import assembly, methods, trees
-
-    rng = np.random.default_rng(seed)
-    pts = rng.random((n, 3))
-    pts = pts[trees.morton_order(pts)]
-    tree = trees.build_tree(pts, depth=depth, root_center=[0.5] * 3, root_halfsize=0.5)
-    core = methods.interpolation_core(tree, methods.laplace, p, nodes="equispaced",
-                                      couplings="toeplitz", transfers="dense", near="none",
-                                      precision=precision)
-    assembly.near_blocks_device(core, "laplace", device=device)
-    return h2, core
-
-
-def launches_per_step(core, mode: int, nrhs: int = 1) -> int:
-    """Kernels one h2b_matvec enqueues (same node-list logic as the library)."""
-    agg = core.plans.trial if mode == 0 else core.plans.test
-    dis = core.plans.test if mode == 0 else core.plans.trial
-    tree = core.trial if mode == 0 else core.test
-    dtree = core.test if mode == 0 else core.trial
-    count = 1  # near
-    if core.field == "real" and nrhs >= 8:
-        count += 1  # gather of the x rows for the tensor-core near kernel
-    count += 1  # leaf aggregation
-    for st in range(agg.agg_level.size):
-        nodes = agg.agg_node[agg.agg_ptr[st]:agg.agg_ptr[st + 1]]
-        if any(not tree.isleaf(int(n)) for n in nodes):
-            count += 1
-    toep = core.coupling_kind == "toeplitz"
-    count += 1 + (2 if toep else 0)  # i2o (+ fft in / out)
-    for st in range(dis.dis_level.size):
-        nodes = dis.dis_node[dis.dis_ptr[st]:dis.dis_ptr[st + 1]]
-        if any(int(n) != 0 and dis.dis_isnode[dtree.parent[int(n)]] for n in nodes):
-            count += 1
-    count += 1  # leaf disaggregation
-    return count
 
 
 class ClockSampler:
@@ -181,151 +156,6 @@ def time_loop(torch, fn, steps, warmup, stream):
     return per, ev[0].elapsed_time(ev[steps])
 
 
-def max_over_ranks(torch, values, world, device):
-    """Each value's maximum over the replicas (the job time is the slowest rank's)."""
-    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return [float(v) for v in t.cpu()]
-
-
-def job_rate(units_per_rank, world, total_ms):
-    """Whole-job throughput of `world` replicas that each processed `units_per_rank` units."""
-    return units_per_rank * world / (total_ms * 1e-3)
-
-
-def pct(v, q):
-    return float(np.percentile(np.asarray(v), q))
-
-
-# ---------------------------------------------------------------------------------------------
-# CPU arms
-# ---------------------------------------------------------------------------------------------
-def cpu_matvec_rate(core, seconds=15.0, nthreads=0):
-    """The oracle (a CPU port of the reference algorithm) on the host cores: RHS/s over a bounded
-    number of forward/transpose matvecs of the full workload."""
-    sys.path.insert(0, ROOT)
-    from oracle import oracle
-    from h2factory_b200.core import flatten
-
-    desc = flatten(core)
-    threads = nthreads or oracle.max_threads()
-    rng = np.random.default_rng(1)
-    x = rng.standard_normal(core.trial.npoints)
-    oracle.matvec(core, x, 0, nthreads=threads, desc=desc)  # warm
-    done, t0, times = 0, time.perf_counter(), []
-    while time.perf_counter() - t0 < seconds or done < 2:
-        t1 = time.perf_counter()
-        oracle.matvec(core, x, done % 2, nthreads=threads, desc=desc)
-        times.append(time.perf_counter() - t1)
-        done += 1
-    wall = time.perf_counter() - t0
-    return {"value": done / wall, "unit": "RHS/s", "cores": threads, "kind": "port",
-            "sample": f"{done} full matvecs (alternating forward/transpose, 1 RHS) in {wall:.1f} s",
-            "p50_ms": pct(times, 50) * 1e3, "p99_ms": pct(times, 99) * 1e3}
-
-
-def reference_arm(args, rank, world):
-    if rank != 0:
-        return
-    import torch
-
-    device = "cuda:0" if torch.cuda.is_available() else "cpu"
-    if device == "cpu":
-        h2, core = build_core_cpu()
-    else:
-        h2, core = build_core(device=device)
-        core.near_data = core.near_device.cpu().numpy()
-        core.near_device = None
-        torch.cuda.empty_cache()
-    per = max(1, args.steps)
-    sys.path.insert(0, ROOT)
-    from oracle import oracle
-    from h2factory_b200.core import flatten
-
-    desc = flatten(core)
-    threads = oracle.max_threads()
-    rng = np.random.default_rng(1)
-    x = rng.standard_normal(core.trial.npoints)
-    for i in range(args.warmup):
-        oracle.matvec(core, x, i % 2, nthreads=threads, desc=desc)
-    times = []
-    for i in range(per):
-        t1 = time.perf_counter()
-        oracle.matvec(core, x, i % 2, nthreads=threads, desc=desc)
-        times.append(time.perf_counter() - t1)
-    tot = sum(times)
-    value = per / tot
-    line = {"metric": METRIC, "value": value, "unit": "RHS/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": per, "warmup": args.warmup, "ms_per_step": tot / per * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "rhs_per_step": 1, "modes": "forward/transpose alternating"},
-            "p50_ms": pct(times, 50) * 1e3, "p99_ms": pct(times, 99) * 1e3,
-            "cpu_baseline": {"value": value, "unit": "RHS/s", "cores": threads, "kind": "port",
-                             "sample": f"{per} full matvecs of the workload after {args.warmup} warm-up"},
-            "e2e": {"value": value, "unit": "RHS/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference is Julia and cannot run here; this arm times the C restatement of its "
-                    "CPU algorithm (oracle/) with OpenMP over node chunks"}
-    print(json.dumps(line), flush=True)
-
-
-def build_core_cpu():
-    h2 = _package()
-    from h2factory_b200 import methods, trees
-
-    rng = np.random.default_rng(0)
-    pts = rng.random((262144, 3))
-    pts = pts[trees.morton_order(pts)]
-    tree = trees.build_tree(pts, depth=5, root_center=[0.5] * 3, root_halfsize=0.5)
-    core = methods.interpolation_core(tree, methods.laplace, 4, nodes="equispaced", couplings="toeplitz")
-    return h2, core
-
-
-# ---------------------------------------------------------------------------------------------
-# GPU arm
-# ---------------------------------------------------------------------------------------------
-def form_run(torch, h2, core, nrhs, steps, warmup, device, seed):
-    """Time `steps` matvecs (forward/transpose alternating) on an `nrhs` block; device events."""
-    ws = h2.H2Workspace(core, max_nrhs=nrhs, device=int(device.split(":")[1]))
-    n = core.trial.npoints
-    rng = np.random.default_rng(seed)
-    xh = rng.standard_normal((n, nrhs))
-    x = torch.from_numpy(np.ascontiguousarray(xh.T)).to(device).t()
-    ys = [torch.zeros((nrhs, n), dtype=torch.float64, device=device).t() for _ in range(2)]
-    views = [ws, h2.transpose(ws)]
-    stream = torch.cuda.current_stream(device)
-    sptr = stream.cuda_stream
-
-    def step(i):
-        h2.mul_(ys[i % 2], views[i % 2], x, stream=sptr)
-
-    per, total = time_loop(torch, step, steps, warmup, stream)
-    return ws, x, xh, per, total
-
-
-def served_run(torch, h2, core, nrhs, steps, warmup, device, seed, inflight):
-    """The served form: `steps` requests of `nrhs` right-hand sides, forward/transpose alternating,
-    `inflight` of them on the device at once (request i on workspace and stream i % inflight, as a
-    serving loop runs them). Device events: per-request latency on its stream, and the total from
-    one start event that every stream waits for to the last request's end."""
-    dcore = h2.DeviceCore(core, int(device.split(":")[1]))  # one resident core, one workspace per request slot
-    wss = [h2.H2Workspace(dcore, max_nrhs=nrhs) for _ in range(inflight)]
-    n = core.trial.npoints
-    rng = np.random.default_rng(seed)
-    xh = rng.standard_normal((n, nrhs))
-    x = torch.from_numpy(np.ascontiguousarray(xh.T)).to(device).t()
-    ys = [torch.zeros((nrhs, n), dtype=torch.float64, device=device).t() for _ in range(inflight)]
-    streams = [torch.cuda.Stream(device) for _ in range(inflight)]
-    views = [[w, h2.transpose(w)] for w in wss]
-
-    def enqueue(i):
-        j = i % inflight
-        h2.mul_(ys[j], views[j][i % 2], x, stream=streams[j].cuda_stream)
-
-    per, total = time_streams(torch, enqueue, steps, warmup, streams, device)
-    return wss, x, xh, per, total
-
-
 def time_streams(torch, enqueue, steps, warmup, streams, device):
     """Per-request device times (ms) and the total of `steps` requests spread over `streams`."""
     for i in range(warmup):
@@ -349,187 +179,505 @@ def time_streams(torch, enqueue, steps, warmup, streams, device):
     return [a.elapsed_time(b) for a, b in ev], t0.elapsed_time(t1)
 
 
-def gpu_arm(args, rank, world, local_rank):
-    import copy
+def max_over_ranks(torch, values, world, device):
+    """Each value's maximum over the replicas (the job time is the slowest rank's)."""
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
 
+
+def job_rate(units_per_rank, world, total_ms):
+    """Whole-job throughput of `world` replicas that each processed `units_per_rank` units."""
+    return units_per_rank * world / (total_ms * 1e-3)
+
+
+def pct(v, q):
+    return float(np.percentile(np.asarray(v), q))
+
+
+# ---------------------------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------------------------
+def sphere_points(n, seed=0):
+    """Fibonacci lattice on the unit sphere with seeded jitter of 0.1 x spacing, scaled to radius
+    0.45 about the centre of the unit cube."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n) + 0.5
+    phi, th = np.arccos(1 - 2 * i / n), np.pi * (1 + 5 ** 0.5) * i
+    p = np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], axis=1)
+    p = p + 0.1 * np.sqrt(4 * np.pi / n) * rng.standard_normal(p.shape)
+    return 0.5 + 0.45 * p
+
+
+def sphere_core(n, device, precision="fp64", transfers="separable", near="device"):
+    """The sphere configuration's map at `n` points: leaves <= 128 points, Helmholtz k = 8 pi x 0.45,
+    Chebyshev p = 6, symmetry-reduced couplings, near blocks assembled on the device (or on the host
+    with near="host", for CPU-only runs)."""
+    h2 = _package()
+    from h2factory_b200 import assembly, methods, trees
+
+    tree = trees.build_tree(sphere_points(n), maxvalues=128, root_center=[0.5] * 3, root_halfsize=0.5)
+    core = methods.interpolation_core(tree, methods.helmholtz(SPHERE_K), 6, symmetry=True, precision=precision,
+                                      transfers=transfers, near="host" if near == "host" else "none")
+    if near == "device":
+        assembly.near_blocks_device(core, "helmholtz", wavenumber=SPHERE_K, device=device)
+    return h2, core
+
+
+def toeplitz_core(n=262144, depth=5, p=4, seed=0, device="cuda:0", near="device"):
+    """The Toeplitz configuration's map: Laplace, n points uniform in the unit cube (Morton ordered),
+    uniform octree of `depth`, equispaced p = 4 with FFT'd Toeplitz couplings."""
+    h2 = _package()
+    from h2factory_b200 import assembly, methods, trees
+
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n, 3))
+    pts = pts[trees.morton_order(pts)]
+    tree = trees.build_tree(pts, depth=depth, root_center=[0.5] * 3, root_halfsize=0.5)
+    core = methods.interpolation_core(tree, methods.laplace, p, nodes="equispaced", couplings="toeplitz",
+                                      transfers="dense", near="host" if near == "host" else "none")
+    if near == "device":
+        assembly.near_blocks_device(core, "laplace", device=device)
+    return h2, core
+
+
+def core_with_host_near(core, near_host):
+    c = copy.copy(core)
+    c.near_data, c.near_device = near_host, None
+    return c
+
+
+def fp32_twin(core):
+    c = copy.copy(core)
+    c.precision = "fp32"
+    return c
+
+
+def direct_rows(torch, pts, rows, x, wavenumber, chunk=64):
+    """FP64 direct sum of the kernel rows `rows` against every column: K[rows, :] x on the device."""
+    out = []
+    for s in range(0, rows.numel(), chunk):
+        r = torch.cdist(pts[rows[s:s + chunk]], pts, compute_mode="donot_use_mm_for_euclid_dist")
+        safe = torch.where(r > 0, r, torch.ones_like(r))
+        if wavenumber:
+            k = torch.where(r > 0, torch.exp(1j * wavenumber * safe) / (4 * math.pi * safe),
+                            torch.zeros_like(r, dtype=torch.complex128))
+        else:
+            k = torch.where(r > 0, 1.0 / (4 * math.pi * safe), torch.zeros_like(r))
+        out.append(k.to(x.dtype) @ x)
+        del r, safe, k
+    return torch.cat(out)
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU timing helpers
+# ---------------------------------------------------------------------------------------------
+def _view(h2, ws, mode):
+    return ws if mode == 0 else (h2.transpose(ws) if mode == 1 else h2.adjoint(ws))
+
+
+def requests_run(torch, h2, dcore, nrhs, steps, warmup, device, seed, inflight, modes):
+    """`steps` requests of `nrhs` right-hand sides, orientation modes[i % len(modes)], `inflight`
+    of them on the device at once (request i on workspace and stream i % inflight). Device events:
+    per-request latency on its stream, and the total from one start event to the last end."""
+    wss = [h2.H2Workspace(dcore, max_nrhs=nrhs) for _ in range(inflight)]
+    n = dcore.core.size[1]
+    cplx = dcore.core.field == "complex"
+    dt = torch.complex128 if cplx else torch.float64
+    g = torch.Generator(device=device).manual_seed(seed)
+    x = torch.randn((nrhs, n), dtype=dt, device=device, generator=g).t()
+    ys = [torch.zeros((nrhs, n), dtype=dt, device=device).t() for _ in range(inflight)]
+    streams = [torch.cuda.Stream(device) for _ in range(inflight)]
+    views = [[_view(h2, w, m) for m in modes] for w in wss]
+
+    def enqueue(i):
+        j = i % inflight
+        h2.mul_(ys[j], views[j][i % len(modes)], x, stream=streams[j].cuda_stream)
+
+    per, total = time_streams(torch, enqueue, steps, warmup, streams, device)
+    return wss, x, per, total
+
+
+def e2e_run(torch, wss, nrhs, steps, modes, seed):
+    """The same requests through the host-buffer call (h2b_matvec_host_async) with pinned host
+    buffers, one workspace and stream per request in flight; host wall clock from the first enqueue
+    to the last copy out, plus per-request device times."""
+    inflight = len(wss)
+    core = wss[0].core
+    n = core.size[1]
+    dt = core.dtype
+    device = f"cuda:{wss[0].dcore.device}"
+    rng = np.random.default_rng(seed)
+    xh = rng.standard_normal((n, nrhs))
+    if dt == np.complex128:
+        xh = xh + 1j * rng.standard_normal((n, nrhs))
+    tdt = torch.complex128 if dt == np.complex128 else torch.float64
+    xpin = [torch.from_numpy(np.asfortranarray(xh)).pin_memory().numpy() for _ in range(inflight)]
+    ypin = [torch.zeros((nrhs, n), dtype=tdt).pin_memory().numpy().T for _ in range(inflight)]
+    streams = [torch.cuda.Stream(device) for _ in range(inflight)]
+
+    def host_request(i):
+        j = i % inflight
+        wss[j].matvec_host_async(xpin[j], ypin[j], modes[i % len(modes)], stream=streams[j].cuda_stream)
+
+    for i in range(max(3, inflight)):
+        host_request(i)
+    torch.cuda.synchronize()
+    per, _ = time_streams(torch, host_request, steps, 0, streams, device)
+    t1 = time.perf_counter()
+    for i in range(steps):
+        host_request(i)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t1
+    nbytes = int(n * nrhs * (16 if dt == np.complex128 else 8))
+    return {"value": nrhs * steps / wall, "unit": "RHS/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+            "requests_in_flight": inflight, "clock": "host wall clock, enqueue to last copy out",
+            "steps": steps, "p50_ms": pct(per, 50), "p99_ms": pct(per, 99)}
+
+
+def pass_times(h2, ws, x, modes, reps):
+    """Average device time (ms) of each pass kind over `reps` profiled products per orientation
+    (h2b_profile_matvec: CUDA events on the launching stream, passes serialised), and the number
+    of far-pass launches per product."""
+    acc, nfar = {}, 0
+    for m in modes:
+        for _ in range(reps):
+            recs = h2.profilemul(_view(h2, ws, m), x)
+            nfar = max(nfar, len(recs) - 1)
+            per = {}
+            for r in recs:
+                per[r["pass"]] = per.get(r["pass"], 0.0) + r["ms"]
+            for k, v in per.items():
+                acc.setdefault(k, []).append(v)
+    return {k: float(np.mean(v)) for k, v in acc.items()}, nfar
+
+
+def near_launches(field, nrhs):
+    """Kernels one stored-block near product launches (the dispatch of h2b_near.cu)."""
+    n, r = 0, nrhs
+    if field == "complex":
+        while r >= 8:
+            n += 2          # gather + tensor-core slab kernel per 16 right-hand sides
+            r -= min(16, r)
+        return n + (r + 15) // 16
+    if nrhs >= 8:
+        return 2 * ((nrhs + 15) // 16)
+    return (nrhs + 15) // 16
+
+
+def i2o_useful_flops(core, nrhs):
+    """Real floating-point operations of one dense I2O pass: every far pair (r, t) is an
+    ncoef(r) x ncoef(t) block times nrhs columns; a complex multiply-add is 8 flops."""
+    far = core.plans.far
+
+    def ncoef(sh, tree, nodes):
+        lv = tree.level[nodes]
+        return sh[lv, 0].astype(np.int64) * sh[lv, 1] * sh[lv, 2]
+
+    per = ncoef(core.shape_test, core.test, far[:, 0]) * ncoef(core.shape_trial, core.trial, far[:, 1])
+    return float(per.sum()) * nrhs * (8 if core.field == "complex" else 2)
+
+
+# ---------------------------------------------------------------------------------------------
+# the sphere configuration (headline)
+# ---------------------------------------------------------------------------------------------
+def sphere_leg(args, rank, world, local_rank):
     import torch
 
-    torch.cuda.set_device(local_rank)
-    device = f"cuda:{local_rank}"
-    h2, core = build_core(n=args.n, depth=args.depth, device=device, precision="fp64")
-    core32 = copy.copy(core)
-    core32.precision = "fp32"
-    n = core.trial.npoints
-    nserve = args.nrhs
-    sptr = torch.cuda.current_stream(device).cuda_stream
+    h2 = _package()
+    from h2factory_b200.core import flatten
 
-    # accuracy, before timing: plain FP64 against the CPU oracle and the dense kernel; served FP32
-    # far field against the FP64 GPU product on the same right-hand-side block
+    device = f"cuda:{local_rank}"
+    q = args.nrhs
+    modes = (0, 2)  # forward / adjoint
+    t_build = time.perf_counter()
+    _, core = sphere_core(args.n, device, transfers=args.transfers)
+    core32 = fp32_twin(core)
+    n = core.trial.npoints
+    d64 = h2.DeviceCore(core, local_rank)
+    d32 = h2.DeviceCore(core32, local_rank)
+    near_host = core.near_device.cpu().numpy() if (rank == 0 and not args.skip_check) else None
+    core.near_device = core32.near_device = None  # each device core holds its own copy
+    torch.cuda.empty_cache()
+    build_s = time.perf_counter() - t_build
+
+    # ---- accuracy, before timing ----
     acc, cpu = {}, None
-    ws64 = h2.H2Workspace(core, max_nrhs=nserve, device=local_rank)
-    ws32 = h2.H2Workspace(core32, max_nrhs=nserve, device=local_rank)
+    ws64 = h2.H2Workspace(d64, max_nrhs=q)
+    ws32 = h2.H2Workspace(d32, max_nrhs=q)
     rng = np.random.default_rng(100 + rank)
-    xb = rng.standard_normal((n, nserve))
+    xb = rng.standard_normal((n, q)) + 1j * rng.standard_normal((n, q))
     xd = torch.from_numpy(np.ascontiguousarray(xb.T)).to(device).t()
-    errs = []
-    for mode, (a64, a32) in enumerate(((ws64, ws32), (h2.transpose(ws64), h2.transpose(ws32)))):
-        y64 = torch.zeros((nserve, n), dtype=torch.float64, device=device).t()
-        y32 = torch.zeros((nserve, n), dtype=torch.float64, device=device).t()
-        h2.mul_(y64, a64, xd, stream=sptr)
-        h2.mul_(y32, a32, xd, stream=sptr)
+    sptr = torch.cuda.current_stream(device).cuda_stream
+    errs, y_fwd = [], None
+    for m in modes:
+        y64 = torch.zeros((q, n), dtype=torch.complex128, device=device).t()
+        y32 = torch.zeros((q, n), dtype=torch.complex128, device=device).t()
+        h2.mul_(y64, _view(h2, ws64, m), xd, stream=sptr)
+        h2.mul_(y32, _view(h2, ws32, m), xd, stream=sptr)
         torch.cuda.synchronize()
-        d = (y32 - y64).norm(dim=0) / y64.norm(dim=0)
-        errs.append(float(d.max()))
+        errs.append(float(((y32 - y64).norm(dim=0) / y64.norm(dim=0)).max()))
+        if m == 0:
+            y_fwd = (y64, y32)
     acc["served_max_rel_err_vs_fp64"] = max(errs)
     if rank == 0 and not args.skip_check:
+        # method error: rows of the FP64 direct sum over all N columns, on the device
+        rows = torch.from_numpy(rng.choice(n, args.dense_rows, replace=False)).to(device)
+        pts = torch.from_numpy(core.test.points).to(device)
+        exact = direct_rows(torch, pts, rows, xd, SPHERE_K)
+        for name, y in (("plain", y_fwd[0]), ("served", y_fwd[1])):
+            acc[f"{name}_rel_err_vs_dense_{args.dense_rows}rows"] = float((y[rows] - exact).norm() / exact.norm())
+        del exact, pts
+        torch.cuda.empty_cache()
+        # the CPU port of the reference algorithm on the same map, one right-hand side: parity of
+        # the plain form and the CPU baseline (the port's loops do not amortise right-hand sides)
         sys.path.insert(0, ROOT)
         from oracle import oracle
 
-        near_host = core.near_device.cpu().numpy()
         hc = core_with_host_near(core, near_host)
-        want = oracle.matvec(hc, xb[:, 0], 0)
-        y0 = torch.zeros(n, dtype=torch.float64, device=device)
-        h2.mul_(y0, ws64, xd[:, 0].contiguous(), stream=sptr)
-        got = y0.cpu().numpy()
-        acc["plain_rel_err_vs_fp64_oracle"] = float(np.linalg.norm(got - want) / np.linalg.norm(want))
-        rows = rng.choice(n, 512, replace=False)
-        P = torch.from_numpy(core.test.points).to(device)
-        dd = P[torch.from_numpy(rows).to(device)][:, None, :] - P[None, :, :]
-        r = torch.sqrt((dd * dd).sum(-1))
-        K = torch.where(r > 0, 1.0 / (4 * np.pi * torch.where(r > 0, r, torch.ones_like(r))), torch.zeros_like(r))
-        exact = (K @ xd[:, 0].contiguous()).cpu().numpy()
-        acc["method_rel_err_vs_dense_512rows"] = float(np.linalg.norm(got[rows] - exact) / np.linalg.norm(exact))
-        del dd, r, K
-        torch.cuda.empty_cache()
-        cpu = cpu_matvec_rate(hc, seconds=args.cpu_seconds)
-        del near_host, hc
+        desc = flatten(hc)
+        threads = oracle.max_threads()
+        t1 = time.perf_counter()
+        want = oracle.matvec(hc, xb[:, 0], 0, nthreads=threads, desc=desc)
+        cpu_s = time.perf_counter() - t1
+        got64 = y_fwd[0][:, 0].cpu().numpy()
+        got32 = y_fwd[1][:, 0].cpu().numpy()
+        acc["plain_rel_err_vs_fp64_oracle"] = float(np.linalg.norm(got64 - want) / np.linalg.norm(want))
+        acc["served_rel_err_vs_fp64_oracle"] = float(np.linalg.norm(got32 - want) / np.linalg.norm(want))
+        cpu = {"value": 1.0 / cpu_s, "unit": "RHS/s", "cores": threads, "kind": "port",
+               "sample": f"one full forward matvec of the workload with 1 right-hand side ({cpu_s:.1f} s; the "
+                         "port's loops do not amortise right-hand sides, so RHS/s = 1 / matvec time)"}
+        del desc, hc, near_host, want
+    del y_fwd
     ws64.close()
     ws32.close()
+    torch.cuda.empty_cache()
     if world > 1:
         torch.distributed.barrier()
 
+    # ---- timed region: plain, served, and both end to end ----
     with ClockSampler(local_rank) as clk:
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
-        wsp, xp, xhp, per_p, tot_p = form_run(torch, h2, core, 1, args.steps, args.warmup, device, 7 + rank)
-        wsl, xs_, xhs, per_s, tot_s = served_run(torch, h2, core32, nserve, args.steps, args.warmup, device,
-                                                 11 + rank, args.inflight)
+        wsp, xpd, per_p, tot_p = requests_run(torch, h2, d64, q, args.steps, args.warmup, device, 7 + rank, 1, modes)
+        wss, xsd, per_s, tot_s = requests_run(torch, h2, d32, q, args.steps, args.warmup, device, 11 + rank,
+                                              args.inflight, modes)
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
-        # dominant kernel: near field, timed alone on the same stream (plain form, 1 RHS)
-        yn = torch.zeros(n, dtype=torch.float64, device=device)
-        xn = xp[:, 0].contiguous()
-        nper, ntotal = time_loop(torch, lambda i: h2.nearmul_(yn, wsp, xn, stream=sptr),
-                                 max(args.steps, 5), 3, torch.cuda.current_stream(device))
+        e2e = e2e_run(torch, wss, q, args.steps, modes, 13 + rank)
+        e2e_plain = e2e_run(torch, wsp, q, max(3, args.steps // 2), modes, 17 + rank)
     tot_p, tot_s = max_over_ranks(torch, [tot_p, tot_s], world, device)
 
-    # end to end through the host-buffer C-ABI call (pinned host memory, copies inside the region):
-    # each request copies its x block in and its y block out; with `inflight` workspaces on their
-    # own streams (h2b_matvec_host_async) one request's copies overlap another's product
-    streams = [torch.cuda.Stream(device) for _ in range(args.inflight)]
-    xpin = [torch.from_numpy(np.asfortranarray(xhs)).pin_memory().numpy() for _ in range(args.inflight)]
-    ypin = [torch.zeros((nserve, n), dtype=torch.float64).pin_memory().numpy().T for _ in range(args.inflight)]
-
-    def host_request(i):
-        j = i % args.inflight
-        wsl[j].matvec_host_async(xpin[j], ypin[j], i % 2, stream=streams[j].cuda_stream)
-
-    for i in range(3):
-        host_request(i)
-    torch.cuda.synchronize()
-    te_dev, _ = time_streams(torch, host_request, args.steps, 0, streams, device)
-    t1 = time.perf_counter()
-    for i in range(args.steps):
-        host_request(i)
-    torch.cuda.synchronize()
-    te_total = time.perf_counter() - t1
-
-    serving = serving_leg(torch, h2, core32, local_rank, args) if args.serve_seconds > 0 else None
-
-    # the serving autotuner's choice for this map (block width, requests in flight), timed on the
-    # resident core; informational: the timed forms above use --nrhs and --inflight
-    tuned = None
-    if args.autotune:
-        from h2factory_b200 import autotune
-
-        tuner = autotune.Autotuner(measure=lambda c, b, f: autotune.measure_on_device(
-            c, b, f, steps=12, warmup=2, device=local_rank, dcore=wsl[0].dcore))
-        ch = tuner.choose(core32, nserve, blocks=(1, 4, 8, 16), inflight=(1, 2, 3))
-        tuned = {"key": ch["key"], "block": ch["block"], "inflight": ch["inflight"],
-                 "rhs_per_s": ch["rhs_per_s"], "p99_ms": ch["p99_ms"],
-                 "trials": [(t["block"], t["inflight"], round(t["rhs_per_s"]), round(t["p99_ms"], 3))
-                            for t in ch["trials"]]}
-
-    # the same map with a matrix-free near field (entries recomputed from the points, no stored
-    # blocks): its own form, reported beside the stored-block forms
-    mf = None
-    if args.matrix_free:
-        free = copy.copy(core)
-        free.set_near_kernel("laplace")
-        free32 = copy.copy(free)
-        free32.precision = "fp32"
-        steps_mf = max(3, args.steps // 10)
-        wfp, _, _, _, tfp = form_run(torch, h2, free, 1, steps_mf, args.warmup, device, 7 + rank)
-        wfs, _, _, _, tfs = form_run(torch, h2, free32, nserve, steps_mf, args.warmup, device, 11 + rank)
-        tfp, tfs = max_over_ranks(torch, [tfp, tfs], world, device)
-        mf = {"plain_rhs_per_s": job_rate(steps_mf, world, tfp), "served_rhs_per_s": job_rate(steps_mf * nserve, world, tfs),
-              "steps": steps_mf, "near_bytes_stored": 0, "device_bytes": int(wfp.dcore.info().device_bytes)}
-        for w in (wfp, wfs):
-            w.close()
-            w.dcore.close()
-
+    # ---- dominant kernels, timed alone on the launching stream ----
+    served_passes, nfar = pass_times(h2, wss[0], xsd, modes, args.profile_reps)
+    plain_passes, _ = pass_times(h2, wsp[0], xpd, modes, args.profile_reps)
     if rank != 0:
-        return
-    hbm, peak_kind = peaks()
-    info = wsp.dcore.info()
-    near_bytes = info.near_entries * 8 + 2 * n * 8
-    near_ms = ntotal / len(nper)
-    achieved = near_bytes / (near_ms * 1e-3) / 1e9
-    workload = WORKLOAD if (args.n, args.depth) == (262144, 5) else f"toeplitz-laplace-N{args.n}-depth{args.depth}-p4"
-    traffic = traffic_table().get(("near_rows_kernel", workload))
-    launches = sum(launches_per_step(core, i % 2, 1) + launches_per_step(core, i % 2, nserve)
-                   for i in range(args.steps))
-    plain_rate = job_rate(args.steps, world, tot_p)
-    served_rate = job_rate(args.steps * nserve, world, tot_s)
+        return None
+    hbm, bf16, peak_kind = peaks()
+    info64 = d64.info()
+    i2o_flops = i2o_useful_flops(core, q)
+    i2o_ms = served_passes["i2o"]
+    i2o_tf = i2o_flops / (i2o_ms * 1e-3) / 1e12
+    near_entries = int(info64.near_entries)
+    near_bytes = near_entries * 16 + 2 * n * q * 16
+    near_ms = plain_passes["near"]
+    near_flops = near_entries * q * 8.0
+    wl = f"sphere-helmholtz-cheb6-N{n}"
+    per_step = nfar + near_launches("complex", q)
+    e2e_steps = args.steps + max(3, args.inflight) + max(3, args.steps // 2) + 3
+    launches = per_step * (2 * args.steps + e2e_steps)
+    plain_rate = job_rate(args.steps * q, world, tot_p)
+    served_rate = job_rate(args.steps * q, world, tot_s)
     line = {
         "metric": METRIC, "value": served_rate, "unit": "RHS/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_s / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 far / f64 near",
-        "data": "synthetic (seeded uniform points in the unit cube)",
-        "config": {"workload": workload, "form": "served: FP32 far field, FP64 near field and sum, "
-                   f"{nserve} right-hand sides coalesced per matvec, {args.inflight} requests in flight",
-                   "rhs_per_step": nserve,
-                   "modes": "forward/transpose alternating", "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (3.2 GB near blocks); no flush",
-                   "near_entries": int(info.near_entries), "i2o_pairs": int(info.npairs[0])},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 far / c128 near",
+        "data": "synthetic (seeded Fibonacci sphere with jitter, complex Gaussian right-hand sides)",
+        "config": {"workload": wl, "kernel": "Helmholtz exp(ik|x-y|)/(4 pi |x-y|), k = 8 pi x 0.45",
+                   "points": n, "leaf_max": 128, "order": 6, "transfers": args.transfers,
+                   "couplings": "dense, symmetry-reduced", "rhs_per_step": q, "modes": "forward/adjoint alternating",
+                   "form": f"served: ComplexF32 far field (tcgen05 TF32-split M2L), FP64 near field and sum, "
+                           f"{q} right-hand sides per request, {args.inflight} requests in flight",
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (17.8 GB near blocks); no flush",
+                   "near_entries": near_entries, "i2o_pairs": int(info64.npairs[0]), "build_s": round(build_s, 1)},
         "p50_ms": pct(per_s, 50), "p99_ms": pct(per_s, 99),
-        "plain": {"value": plain_rate, "unit": "RHS/s", "dtype": "f64", "rhs_per_step": 1,
-                  "ms_per_step": tot_p / args.steps, "p50_ms": pct(per_p, 50), "p99_ms": pct(per_p, 99)},
+        "plain": {"value": plain_rate, "unit": "RHS/s", "dtype": "c128", "rhs_per_step": q,
+                  "ms_per_step": tot_p / args.steps, "p50_ms": pct(per_p, 50), "p99_ms": pct(per_p, 99),
+                  "e2e": e2e_plain},
         "served_over_plain": served_rate / plain_rate,
         "accuracy": acc,
-        "e2e": {"value": nserve * args.steps / te_total, "unit": "RHS/s",
-                "h2d_bytes_per_step": int(n * 8 * nserve), "d2h_bytes_per_step": int(n * 8 * nserve),
-                "requests_in_flight": args.inflight, "clock": "host wall clock, enqueue to last copy out",
-                "p50_ms": pct(te_dev, 50), "p99_ms": pct(te_dev, 99)},
-        "roofline": {"kernel": "near_rows_kernel", "bound": "hbm", "achieved": achieved,
-                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes": near_bytes, "avg_launch_ms": near_ms},
+        "e2e": e2e,
+        "roofline": {"kernel": "i2o_umma_kernel<cfloat> (served form's dense M2L: tcgen05 kind::tf32, three-term split)",
+                     "bound": "tensor", "achieved": i2o_tf, "peak": bf16, "unit": "TFLOP/s", "frac": i2o_tf / bf16,
+                     "peak_kind": f"{peak_kind} dense bf16 (burst)",
+                     "traffic": traffic_table().get(("i2o_umma_kernel", wl)),
+                     "algorithmic_flops": i2o_flops, "avg_launch_ms": i2o_ms,
+                     "issued_tf32_tflops": 3 * i2o_tf, "frac_issued_vs_half_bf16": 3 * i2o_tf / (bf16 / 2)},
+        "roofline_near": {"kernel": "near_slab_mma_c_kernel (FP64 tensor cores; plain and served forms)",
+                          "bound": "fp64 tensor", "achieved_tflops": near_flops / (near_ms * 1e-3) / 1e12,
+                          "achieved_gbs": near_bytes / (near_ms * 1e-3) / 1e9, "hbm_peak": hbm,
+                          "algorithmic_bytes": near_bytes, "algorithmic_flops": near_flops, "avg_ms": near_ms,
+                          "passes_over_blocks": (q + 15) // 16},
+        "passes_ms": {"served": served_passes, "plain": plain_passes},
         "clocks": clk.summary(),
         "gpu_launches": launches,
     }
-    if mf is not None:
-        line["matrix_free_near"] = mf
-    if cpu is not None:
-        line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
-    if serving is not None:
-        line["serving"] = serving
-    if tuned is not None:
-        line["autotune"] = tuned
+    if cpu:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+# ---------------------------------------------------------------------------------------------
+# the Toeplitz configuration
+# ---------------------------------------------------------------------------------------------
+def toeplitz_leg(args, rank, world, local_rank, n=262144, depth=5, nrhs=16, inflight=3):
+    import torch
+
+    h2 = _package()
+    device = f"cuda:{local_rank}"
+    modes = (0, 1)  # forward / transpose
+    _, core = toeplitz_core(n=n, depth=depth, device=device)
+    core32 = fp32_twin(core)
+    d64 = h2.DeviceCore(core, local_rank)
+    d32 = h2.DeviceCore(core32, local_rank)
+    near_host = core.near_device.cpu().numpy() if (rank == 0 and not args.skip_check) else None
+    core.near_device = core32.near_device = None
+    torch.cuda.empty_cache()
+    acc, cpu = {}, None
+    ws64, ws32 = h2.H2Workspace(d64, max_nrhs=nrhs), h2.H2Workspace(d32, max_nrhs=nrhs)
+    rng = np.random.default_rng(200 + rank)
+    xb = rng.standard_normal((n, nrhs))
+    xd = torch.from_numpy(np.ascontiguousarray(xb.T)).to(device).t()
+    errs, y64f = [], None
+    for m in modes:
+        y64 = torch.zeros((nrhs, n), dtype=torch.float64, device=device).t()
+        y32 = torch.zeros((nrhs, n), dtype=torch.float64, device=device).t()
+        h2.mul_(y64, _view(h2, ws64, m), xd)
+        h2.mul_(y32, _view(h2, ws32, m), xd)
+        torch.cuda.synchronize()
+        errs.append(float(((y32 - y64).norm(dim=0) / y64.norm(dim=0)).max()))
+        if m == 0:
+            y64f = y64
+    acc["served_max_rel_err_vs_fp64"] = max(errs)
+    if near_host is not None:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle
+
+        hc = core_with_host_near(core, near_host)
+        threads = oracle.max_threads()
+        t1 = time.perf_counter()
+        want = oracle.matvec(hc, xb[:, 0], 0, nthreads=threads)
+        cpu_s = time.perf_counter() - t1
+        got = y64f[:, 0].cpu().numpy()
+        acc["plain_rel_err_vs_fp64_oracle"] = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+        cpu = {"value": 1.0 / cpu_s, "unit": "RHS/s", "cores": threads, "kind": "port",
+               "sample": f"one forward matvec, 1 right-hand side ({cpu_s:.2f} s)"}
+        del hc, near_host
+    ws64.close()
+    ws32.close()
+    if world > 1:
+        torch.distributed.barrier()
+    wsp, xpd, per_p, tot_p = requests_run(torch, h2, d64, 1, args.steps, args.warmup, device, 7 + rank, 1, modes)
+    wss, xsd, per_s, tot_s = requests_run(torch, h2, d32, nrhs, args.steps, args.warmup, device, 11 + rank,
+                                          inflight, modes)
+    torch.cuda.synchronize()
+    e2e = e2e_run(torch, wss, nrhs, args.steps, modes, 23 + rank)
+    tot_p, tot_s = max_over_ranks(torch, [tot_p, tot_s], world, device)
+    served_passes, _ = pass_times(h2, wss[0], xsd, modes, args.profile_reps)
+    plain_passes, _ = pass_times(h2, wsp[0], xpd, modes, args.profile_reps)
+    if rank != 0:
+        return None
+    hbm, _, peak_kind = peaks()
+    info = d64.info()
+    near_bytes = int(info.near_entries) * 8 + 2 * n * 8
+    near_ms = plain_passes["near"]
+    wl = f"toeplitz-laplace-N{n}-depth{depth}-p4"
+    out = {"workload": wl, "rhs_per_step": nrhs, "modes": "forward/transpose alternating",
+           "served": {"value": job_rate(args.steps * nrhs, world, tot_s), "unit": "RHS/s",
+                      "ms_per_step": tot_s / args.steps, "requests_in_flight": inflight,
+                      "p50_ms": pct(per_s, 50), "p99_ms": pct(per_s, 99), "e2e": e2e},
+           "plain": {"value": job_rate(args.steps, world, tot_p), "unit": "RHS/s", "rhs_per_step": 1,
+                     "ms_per_step": tot_p / args.steps, "p50_ms": pct(per_p, 50), "p99_ms": pct(per_p, 99)},
+           "accuracy": acc,
+           "roofline_near": {"kernel": "near_rows_kernel (plain form, 1 RHS)", "bound": "hbm",
+                             "achieved": near_bytes / (near_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                             "frac": near_bytes / (near_ms * 1e-3) / 1e9 / hbm, "peak_kind": peak_kind,
+                             "traffic": traffic_table().get(("near_rows_kernel", wl)),
+                             "algorithmic_bytes": near_bytes, "avg_launch_ms": near_ms},
+           "passes_ms": {"served": served_passes, "plain": plain_passes},
+           "near_entries": int(info.near_entries), "i2o_pairs": int(info.npairs[0])}
+    out["served_over_plain"] = out["served"]["value"] / out["plain"]["value"]
+    if cpu:
+        out["cpu_baseline"] = cpu
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# reference arm: the CPU port of the reference algorithm on the headline workload
+# ---------------------------------------------------------------------------------------------
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    import torch
+
+    _package()
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    from h2factory_b200.core import flatten
+
+    on_gpu = torch.cuda.is_available()
+    if args.workload == "sphere":
+        _, core = sphere_core(args.n, "cuda:0", transfers=args.transfers, near="device" if on_gpu else "host")
+        modes, wl = (0, 2), f"sphere-helmholtz-cheb6-N{args.n}"
+    else:
+        _, core = toeplitz_core(n=args.n, device="cuda:0", near="device" if on_gpu else "host")
+        modes, wl = (0, 1), f"toeplitz-laplace-N{args.n}-depth5-p4"
+    if core.near_device is not None:
+        core = core_with_host_near(core, core.near_device.cpu().numpy())
+        torch.cuda.empty_cache()
+    desc = flatten(core)
+    threads = oracle.max_threads()
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(core.trial.npoints)
+    if core.field == "complex":
+        x = x + 1j * rng.standard_normal(core.trial.npoints)
+    # warm-up and timed steps are whole 1-RHS matvecs; a step of the sphere map takes seconds, so
+    # the run is bounded: one warm-up, and timed steps until --reference-seconds have passed
+    for i in range(min(args.warmup, 1)):
+        oracle.matvec(core, x, modes[i % 2], nthreads=threads, desc=desc)
+    times, t0 = [], time.perf_counter()
+    for i in range(args.steps):
+        t1 = time.perf_counter()
+        oracle.matvec(core, x, modes[i % 2], nthreads=threads, desc=desc)
+        times.append(time.perf_counter() - t1)
+        if time.perf_counter() - t0 > args.reference_seconds and len(times) >= 2:
+            break
+    tot = sum(times)
+    done = len(times)
+    value = done / tot
+    line = {"metric": METRIC, "value": value, "unit": "RHS/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": done, "steps_requested": args.steps, "warmup": min(args.warmup, 1),
+            "ms_per_step": tot / done * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128" if core.field == "complex" else "f64", "data": "synthetic (seeded)",
+            "config": {"workload": wl, "rhs_per_step": 1,
+                       "modes": "forward/adjoint alternating" if modes[1] == 2 else "forward/transpose alternating"},
+            "p50_ms": pct(times, 50) * 1e3, "p99_ms": pct(times, 99) * 1e3,
+            "cpu_baseline": {"value": value, "unit": "RHS/s", "cores": threads, "kind": "port",
+                             "sample": f"{done} full matvecs of the workload, 1 right-hand side each (the port's "
+                                       f"loops do not amortise right-hand sides), after one warm-up; steps stop "
+                                       f"after {args.reference_seconds:.0f} s"},
+            "e2e": {"value": value, "unit": "RHS/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference is Julia and cannot run here; this arm times the C restatement of its CPU "
+                    "algorithm (oracle/) with OpenMP over node chunks on all host threads"}
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------
+# serving and batched modes
+# ---------------------------------------------------------------------------------------------
 def serving_leg(torch, h2, core, local_rank, args):
     """Closed-loop clients against the continuous-batching server on the served form's map.
 
@@ -540,22 +688,22 @@ def serving_leg(torch, h2, core, local_rank, args):
     from h2factory_b200.serving import GpuExecutor, MatvecServer
 
     device = f"cuda:{local_rank}"
-    srv = MatvecServer(GpuExecutor(local_rank), budget_bytes=150e9, max_block=args.nrhs, slots=2)
-    srv.add_map("toeplitz", core)
+    srv = MatvecServer(GpuExecutor(local_rank), budget_bytes=150e9, max_block=16, slots=2)
+    srv.add_map("map", core)
     n = core.trial.npoints
-    xs = [torch.randn(n, dtype=torch.float64, device=device) for _ in range(args.clients)]
+    dt = torch.complex128 if core.field == "complex" else torch.float64
+    xs = [torch.randn(n, dtype=dt, device=device) for _ in range(args.clients)]
     torch.cuda.synchronize()
-    srv.submit("toeplitz", xs[0]).result(timeout=300)  # load the map and warm the slots
+    srv.submit("map", xs[0]).result(timeout=300)  # load the map and warm the slots
     stop = [False]
     counts = [0] * args.clients
-    t_start = [0.0]
 
     def client(i):
         r = np.random.default_rng(1000 + i)
         while not stop[0]:
             u = r.random()
             mode = "forward" if u < 0.6 else ("transpose" if u < 0.8 else "adjoint")
-            srv.submit("toeplitz", xs[i], mode).result(timeout=300)
+            srv.submit("map", xs[i], mode).result(timeout=300)
             counts[i] += 1
 
     ts = [threading.Thread(target=client, args=(i,), daemon=True) for i in range(args.clients)]
@@ -576,37 +724,8 @@ def serving_leg(torch, h2, core, local_rank, args):
     srv.close()
     return {"clients": args.clients, "mode_mix": "60/20/20 forward/transpose/adjoint",
             "requests": done, "seconds": wall, "rhs_per_s": done / wall, "p50_ms": stats["p50_ms"],
-            "p99_ms": stats["p99_ms"], "mean_block": stats["mean_block"], "max_block": args.nrhs,
+            "p99_ms": stats["p99_ms"], "mean_block": stats["mean_block"], "max_block": 16,
             "requests_on_device": True}
-
-
-def core_with_host_near(core, near_host):
-    import copy
-
-    c = copy.copy(core)
-    c.near_data, c.near_device = near_host, None
-    return c
-
-
-def sphere_core(n, device, precision="fp64", transfers="dense"):
-    """The sphere configuration's map at `n` points: Fibonacci sphere (radius 0.45 in the unit
-    cube) with jitter 0.1 x spacing, leaves <= 128 points, Helmholtz k = 8 pi x 0.45 (the unit
-    sphere's electrical size), Chebyshev p = 6, symmetry-reduced couplings, near blocks assembled
-    on the device."""
-    h2 = _package()
-    from h2factory_b200 import assembly, methods, trees
-
-    rng = np.random.default_rng(0)
-    i = np.arange(n) + 0.5
-    phi, th = np.arccos(1 - 2 * i / n), np.pi * (1 + 5 ** 0.5) * i
-    p = np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], axis=1)
-    p = p + 0.1 * np.sqrt(4 * np.pi / n) * rng.standard_normal(p.shape)
-    tree = trees.build_tree(0.5 + 0.45 * p, maxvalues=128, root_center=[0.5] * 3, root_halfsize=0.5)
-    k = 8 * np.pi * 0.45
-    core = methods.interpolation_core(tree, methods.helmholtz(k), 6, near="none", symmetry=True,
-                                      precision=precision, transfers=transfers)
-    assembly.near_blocks_device(core, "helmholtz", wavenumber=k, device=device)
-    return h2, core
 
 
 def batched_arm(args):
@@ -668,84 +787,69 @@ def batched_arm(args):
     b.close()
 
 
-def sphere_arm(args):
-    """Dense (Chebyshev) far field on the sphere configuration's shape: FP64 and FP32 forms, 32
-    complex right-hand sides per matvec, forward/adjoint alternating (device timing)."""
-    import copy
-
+def gpu_arm(args, rank, world, local_rank):
     import torch
 
-    device = "cuda:0"
-    h2, core = sphere_core(args.n, device, transfers=args.transfers)
-    n = core.trial.npoints
-    stream = torch.cuda.current_stream(device)
-    x = torch.randn((32, n), dtype=torch.complex128, device=device).t()
-    out = {}
-    ref = None
-    for prec in ("fp64", "fp32"):
-        c = copy.copy(core)
-        c.precision = prec
-        ws = h2.H2Workspace(c, max_nrhs=32)
-        y = torch.zeros((32, n), dtype=torch.complex128, device=device).t()
-        views = [ws, h2.adjoint(ws)]
-        per, tot = time_loop(torch, lambda i: h2.mul_(y, views[i % 2], x, stream=stream.cuda_stream),
-                             args.steps, args.warmup, stream)
-        h2.mul_(y, ws, x, stream=stream.cuda_stream)
-        torch.cuda.synchronize()
-        if ref is None:
-            ref = y.clone()
-        out[prec] = {"rhs_per_s": 32 * args.steps / (tot * 1e-3), "ms_per_step": tot / args.steps,
-                     "p50_ms": pct(per, 50), "p99_ms": pct(per, 99),
-                     "rel_err_vs_fp64": float(((y - ref).norm(dim=0) / ref.norm(dim=0)).max())}
-        ws.close()
-        ws.dcore.close()
-    print(json.dumps({
-        "metric": METRIC, "value": out["fp32"]["rhs_per_s"], "unit": "RHS/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": out["fp32"]["ms_per_step"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c64 far / c128 near", "data": "synthetic (seeded sphere)",
-        "config": {"workload": f"sphere-helmholtz-cheb6-N{n}", "rhs_per_step": 32, "modes": "forward/adjoint",
-                   "far_pairs": int(core.plans.far.shape[0]), "near_entries": int(core.near_device.numel()),
-                   "l2": "near blocks larger than L2; no flush"},
-        "fp64": out["fp64"], "fp32": out["fp32"]}))
+    torch.cuda.set_device(local_rank)
+    if args.workload == "sphere":
+        line = sphere_leg(args, rank, world, local_rank)
+        if args.toeplitz_leg:
+            tl = toeplitz_leg(args, rank, world, local_rank)
+            if line is not None:
+                line["toeplitz"] = tl
+    else:
+        tl = toeplitz_leg(args, rank, world, local_rank, n=args.n)
+        line = None
+        if tl is not None:
+            line = {"metric": METRIC, "value": tl["served"]["value"], "unit": "RHS/s", "n_gpus": world,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": tl["served"]["ms_per_step"],
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "f32 far / f64 near", "data": "synthetic (seeded uniform points in the unit cube)",
+                    "config": {"workload": tl["workload"]}, "e2e": tl["served"]["e2e"], "toeplitz": tl}
+    if args.serve_seconds > 0:
+        h2 = _package()
+        _, sc = toeplitz_core(n=args.n if args.workload == "toeplitz" else 262144, device=f"cuda:{local_rank}")
+        serving = serving_leg(torch, h2, fp32_twin(sc), local_rank, args)
+        if line is not None:
+            line["serving"] = serving
+    if line is not None:
+        print(json.dumps(line), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--nrhs", type=int, default=16, help="right-hand sides per served block")
-    ap.add_argument("--inflight", type=int, default=3,
-                    help="served requests on the device at once (3: the autotuner's choice for this map)")
-    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
-                    help="skip the autotuner's report of block width and requests in flight")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--skip-check", action="store_true")
-    ap.add_argument("--n", type=int, default=262144, help="points (smaller cases are for profiling)")
-    ap.add_argument("--depth", type=int, default=5)
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "toeplitz"])
+    ap.add_argument("--n", type=int, default=None, help="points (default: the configuration's size)")
+    ap.add_argument("--nrhs", type=int, default=32, help="right-hand sides per request of the sphere workload")
+    ap.add_argument("--inflight", type=int, default=2, help="served requests on the device at once")
+    ap.add_argument("--transfers", default="separable", choices=["dense", "separable"],
+                    help="level transfers of the sphere map")
+    ap.add_argument("--no-toeplitz", dest="toeplitz_leg", action="store_false",
+                    help="skip the Toeplitz configuration's secondary leg")
+    ap.add_argument("--skip-check", action="store_true", help="skip the oracle / direct-sum checks")
+    ap.add_argument("--dense-rows", type=int, default=4096, help="rows of the FP64 direct-sum check")
+    ap.add_argument("--profile-reps", type=int, default=2, help="profiled products per orientation")
+    ap.add_argument("--reference-seconds", type=float, default=150.0,
+                    help="time budget of the reference arm's timed steps")
     ap.add_argument("--clients", type=int, default=64, help="closed-loop clients of the serving leg")
-    ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving leg length (0: skip)")
-    ap.add_argument("--no-matrix-free", dest="matrix_free", action="store_false",
-                    help="skip the matrix-free near-field forms")
+    ap.add_argument("--serve-seconds", type=float, default=0.0, help="serving leg length (0: skip)")
     ap.add_argument("--batched", action="store_true",
                     help="time the batched-uneven configuration's shape (eager vs one graph replay per pass)")
     ap.add_argument("--maps", type=int, default=96, help="maps of the batched mode")
     ap.add_argument("--nmax", type=int, default=16384, help="largest point count of the batched mode")
-    ap.add_argument("--transfers", default="dense", choices=["dense", "separable"],
-                    help="level transfers of the sphere mode's map")
-    ap.add_argument("--sphere", action="store_true",
-                    help="time the sphere configuration's shape at --n points instead (dense far field)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.n is None:
+        args.n = 1048576 if args.workload == "sphere" else 262144
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank, world)
-        return
-    if args.sphere:
-        sphere_arm(args)
         return
     if args.batched:
         batched_arm(args)
@@ -756,7 +860,7 @@ def main():
         import torch
 
         torch.cuda.set_device(local_rank)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         gpu_arm(args, rank, world, local_rank)
     finally:
