@@ -351,6 +351,114 @@ __device__ void separable_block(const T *M, const int *sp, const int *sc, int di
 }
 
 // ---------------------------------------------------------------------------------------------
+// Separable level transfers (SeparableI2I, src/maps/leveltranslator.jl:168-265) on blocks of
+// right-hand sides: one CTA per parent (upward: m_p = sum over children of op(T_c) m_c, first child
+// overwriting) or per child (downward: l_c (+)= op(T_c)^T l_p, accumulating where the child already
+// received I2O contributions). A chunk of `qc` moment columns is contracted axis by axis in
+// shared memory (axes dim .. 1, one barrier per axis, ping-pong buffers); each thread computes
+// whole output elements of the axis pass, so the work of one barrier is qc times that of one column.
+// ---------------------------------------------------------------------------------------------
+template <class T, bool UP>
+__global__ void __launch_bounds__(256)
+transfer_sep_kernel(DMap m, DSide s, const int *__restrict__ nodes, const uint8_t *__restrict__ received,
+                    bool conjt, int nrhs, T *__restrict__ mom, int qc_max, int bufsz) {
+    using A = typename ScalarTraits<T>::Acc;
+    extern __shared__ unsigned char smem_raw[];
+    A *X = reinterpret_cast<A *>(smem_raw), *Y = X + (size_t)qc_max * bufsz, *Acc = Y + (size_t)qc_max * bufsz;
+    const int node = nodes[blockIdx.x];
+    const int lp = UP ? s.level[node] : s.level[node] - 1, lc = lp + 1;
+    const int *sp = &s.shape[3 * lp], *sc = &s.shape[3 * lc];
+    int fin[3], fout[3];
+    for (int d = 0; d < 3; ++d) {
+        fin[d] = UP ? sc[d] : sp[d];
+        fout[d] = UP ? sp[d] : sc[d];
+    }
+    const int nin = fin[0] * fin[1] * fin[2], nout = fout[0] * fout[1] * fout[2];
+    const int nq = m.ncomp * nrhs;
+    const int c0 = UP ? s.child_ptr[node] : 0, c1 = UP ? s.child_ptr[node + 1] : 1;
+    T *dst = mom + s.mom_off[node] * nrhs;
+    const bool acc_dst = !UP && received[node] != 0;
+    for (int q0 = 0; q0 < nq; q0 += qc_max) {
+        const int qc = min(qc_max, nq - q0);
+        A *res = X;
+        for (int k = c0; k < c1; ++k) {
+            const int ch = UP ? s.child[k] : node;  // the transfer belongs to the child
+            const T *src = UP ? mom + s.mom_off[ch] * nrhs : mom + s.mom_off[s.parent[node]] * nrhs;
+            const T *M = static_cast<const T *>(s.tr) + s.tr_off[lc * m.nsectors + s.sector[ch]];
+            const T *fac[3];
+            int64_t o = 0;
+            for (int d = 0; d < m.dim; ++d) {
+                fac[d] = M + o;
+                o += (int64_t)sp[d] * sc[d];
+            }
+            for (int e = threadIdx.x; e < qc * nin; e += blockDim.x) {
+                const int q = e / nin, i = e - q * nin;
+                X[q * bufsz + i] = wide(src[(int64_t)(q0 + q) * nin + i]);
+            }
+            __syncthreads();
+            int cur[3] = {fin[0], fin[1], fin[2]};
+            A *a = X, *b = Y;
+            for (int ax = m.dim - 1; ax >= 0; --ax) {
+                int nxt[3] = {cur[0], cur[1], cur[2]};
+                nxt[ax] = fout[ax];
+                const int tot = nxt[0] * nxt[1] * nxt[2], ld = sp[ax], kk = cur[ax];
+                const int sstr = ax == 0 ? 1 : (ax == 1 ? cur[0] : cur[0] * cur[1]);  // input stride along ax
+                for (int e = threadIdx.x; e < qc * tot; e += blockDim.x) {
+                    const int q = e / tot, f = e - q * tot;
+                    const int i0 = f % nxt[0], i1 = (f / nxt[0]) % nxt[1], i2 = f / (nxt[0] * nxt[1]);
+                    const int row = ax == 0 ? i0 : (ax == 1 ? i1 : i2);
+                    int base = i0 + cur[0] * (i1 + cur[1] * i2);  // the input index with i[ax] = 0
+                    base -= row * sstr;
+                    const A *in = a + q * bufsz + base;
+                    A acc = sc_zero<A>();
+                    for (int j = 0; j < kk; ++j) {
+                        // up: op(M)[row, j] = M[row + j ld]; down: M^T[row, j] = M[j + row ld]
+                        const T mk = UP ? fac[ax][row + j * ld] : fac[ax][j + row * ld];
+                        acc = acc + wide(cj(mk, conjt)) * in[j * sstr];
+                    }
+                    b[q * bufsz + f] = acc;
+                }
+                __syncthreads();
+                A *t = a;
+                a = b;
+                b = t;
+                cur[0] = nxt[0];
+                cur[1] = nxt[1];
+                cur[2] = nxt[2];
+            }
+            res = a;
+            if (UP && c1 - c0 > 1) {
+                for (int e = threadIdx.x; e < qc * nout; e += blockDim.x) {
+                    const int q = e / nout, i = e - q * nout;
+                    Acc[q * bufsz + i] = (k == c0 ? sc_zero<A>() : Acc[q * bufsz + i]) + a[q * bufsz + i];
+                }
+                res = Acc;
+                __syncthreads();
+            }
+        }
+        for (int e = threadIdx.x; e < qc * nout; e += blockDim.x) {
+            const int q = e / nout, i = e - q * nout;
+            T *o = dst + (int64_t)(q0 + q) * nout + i;
+            narrow(acc_dst ? wide(*o) + res[q * bufsz + i] : res[q * bufsz + i], *o);
+        }
+        __syncthreads();
+    }
+}
+
+template <class T, bool UP>
+cudaError_t launch_transfer_sep(const DMap &m, const DSide &s, const int *nodes, int nnodes, const uint8_t *received,
+                                bool conjt, int nrhs, void *mom, int maxsep, cudaStream_t st) {
+    using A = typename ScalarTraits<T>::Acc;
+    const int nq = m.ncomp * nrhs;
+    // moment columns per chunk: three buffers of maxsep accumulators each within 48 KB
+    const int qc = std::max(1, std::min(nq, (int)((48 * 1024) / (3 * (size_t)maxsep * sizeof(A)))));
+    const size_t sm = 3 * (size_t)qc * maxsep * sizeof(A);
+    transfer_sep_kernel<T, UP><<<nnodes, 256, sm, st>>>(m, s, nodes, received, conjt, nrhs, static_cast<T *>(mom),
+                                                        qc, maxsep);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
 // A2: m_p = sum over children of op(T_{level(c), sector(c)}) m_c, first child overwriting.
 // ---------------------------------------------------------------------------------------------
 template <class T, bool MMA>
@@ -1433,6 +1541,12 @@ cudaError_t launch_transfer_up(bool cplx, int precision, const DMap &m, const DS
     }
     const int bs = m.transfer_kind == H2B_TRANSFER_DENSE ? 256 : block_for(maxcoef);
     cudaError_t err = cudaSuccess;
+    if (m.transfer_kind == H2B_TRANSFER_SEPARABLE) {
+        H2B_DISPATCH_T(cplx, precision, {
+            err = launch_transfer_sep<T, true>(m, s, nodes, nnodes, nullptr, conjt, fa.nrhs, fa.am, maxsep, st);
+        });
+        return err;
+    }
     H2B_DISPATCH_T(cplx, precision, {
         using A = typename ScalarTraits<T>::Acc;
         const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? tile_smem<A>()
@@ -1621,6 +1735,12 @@ cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const 
     const int bs = m.transfer_kind == H2B_TRANSFER_DENSE ? 256 : block_for(maxcoef, 64, 256);
     const bool conjt = fa.mode == H2B_ADJOINT;
     cudaError_t err = cudaSuccess;
+    if (m.transfer_kind == H2B_TRANSFER_SEPARABLE) {
+        H2B_DISPATCH_T(cplx, precision, {
+            err = launch_transfer_sep<T, false>(m, s, nodes, nnodes, received, conjt, fa.nrhs, fa.dm, maxsep, st);
+        });
+        return err;
+    }
     H2B_DISPATCH_T(cplx, precision, {
         using A = typename ScalarTraits<T>::Acc;
         const size_t sm = m.transfer_kind == H2B_TRANSFER_DENSE ? tile_smem<A>()
