@@ -857,6 +857,40 @@ h2b_status build_near(h2b_core *c, const h2b_map_desc &d) {
     return H2B_OK;
 }
 
+// The FP32 form's dense couplings transposed block by block (same offsets), for the tensor-core
+// I2O's transposed and adjoint products, and whether every block is laid out for 16-byte bulk
+// copies of its columns. A block's shape is (receiver coefficients x source coefficients) of the
+// test-side pairs that use it.
+h2b_status build_transposed_couplings(h2b_core *c, const h2b_map_desc &d, const std::vector<int64_t> &off) {
+    const bool cplx = d.field == H2B_COMPLEX;
+    const int fw = cplx ? 2 : 1;
+    const int64_t n = d.coupling_len / fw;  // elements
+    std::vector<int64_t> rows(std::max<int64_t>(d.ncouplings, 1), -1), cols(rows.size(), -1);
+    for (int r = 0; r < d.test.nnodes; ++r)
+        for (int p = d.test.i2o_ptr[r]; p < d.test.i2o_ptr[r + 1]; ++p) {
+            const int64_t k = d.test.i2o_coupling[p];
+            rows[k] = ncoef_host(d.test, d.test.level[r]);
+            cols[k] = ncoef_host(d.trial, d.trial.level[d.test.i2o_src[p]]);
+        }
+    std::vector<double> tr((size_t)std::max<int64_t>(n, 1) * fw, 0.0);
+    const int eb = 4 * fw;  // bytes per FP32 element
+    bool vec = true;
+    std::vector<char> done((size_t)std::max<int64_t>(n, 1), 0);
+    for (int64_t k = 0; k < d.ncouplings; ++k) {
+        if (rows[k] < 0) continue;
+        const int64_t o = off[k], nr = rows[k], nc = cols[k];
+        vec &= (o * eb) % 16 == 0 && (nr * eb) % 16 == 0 && (nc * eb) % 16 == 0;
+        if (done[o]) continue;  // symmetry-reduced couplings share their canonical block
+        done[o] = 1;
+        for (int64_t j = 0; j < nc; ++j)
+            for (int64_t i = 0; i < nr; ++i)
+                for (int w = 0; w < fw; ++w)
+                    tr[(size_t)(o + j + i * nc) * fw + w] = d.coupling[(size_t)(o + i + j * nr) * fw + w];
+    }
+    c->dmap.cpl_vec = vec ? 1 : 0;
+    return upload_far_scalars(c, tr.data(), std::max<int64_t>(n, 1), &c->dmap.cpl_t);
+}
+
 // Padded shape (2s - 1 per axis) of every coupling, from the pairs that use it; 0 if unused.
 std::vector<int> coupling_shapes(const h2b_map_desc &d) {
     std::vector<int> ts(3 * std::max<int64_t>(d.ncouplings, 1), 0);
@@ -944,6 +978,8 @@ h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
         const int fw = cplx ? 2 : 1;
         for (int64_t k = 0; k < d.ncouplings; ++k) off[k] = d.coupling_offset[k] / fw;
         st = upload_far_scalars(c, d.coupling, d.coupling_len / fw, &M.cpl);
+        if (st == H2B_OK && c->precision == H2B_FP32 && d.coupling_kind == H2B_COUPLING_DENSE)
+            st = build_transposed_couplings(c, d, off);
     }
     if (st) return st;
     int64_t *q;

@@ -103,6 +103,12 @@ struct DMap {
     int cube_ts;             // > 0: every level's padded Toeplitz arrays are cube_ts^3 (3-D cubes)
     const int64_t *cpl_off;  // [ncouplings] offsets in elements of T (dense/diag) or spectrum (Toeplitz)
     const void *cpl;
+    // FP32 dense couplings for the tensor-core I2O: every block transposed, at the same offsets,
+    // so that transposed / adjoint products read columns of a stored block like forward ones
+    const void *cpl_t = nullptr;
+    // every dense block starts on a 16-byte boundary and its columns are whole multiples of 16 bytes:
+    // the tensor-core I2O then copies coupling columns with bulk (TMA) copies
+    int cpl_vec = 0;
     // permuted dense couplings: sets [rowperm | rowperm^-1 | colperm | colperm^-1], n entries each
     const int *perm = nullptr;
 };

@@ -7,30 +7,30 @@
 // concatenated pairs: D[nc x nq] = [op(B_1) op(B_2) ...] [m_1; m_2; ...].
 //
 // One CTA per (receiver, 128-row tile of its coefficients, tile of right-hand sides), one CTA per
-// SM, warp-specialised; the K dimension streams in chunks of 16 FP32 values and every hand-off is
-// an mbarrier (no block barrier inside the loop):
+// SM, warp-specialised; the K dimension streams in chunks of 16 FP32 values through UM_NS stages,
+// and every hand-off is an mbarrier (no block barrier inside the loop):
 //   * coupling warps (0-3), one thread per tile row: load the row's 16 values of chunk c + 3 into
-//     a register ring (the couplings are L2-resident), split chunk c into TF32 high parts and
-//     rounded remainders and write them into a tensor-memory stage with tcgen05.st. The MMAs take
-//     this operand (A) straight from tensor memory, so it never passes through shared memory;
-//   * moment warps (4-6): cp.async each chunk's source moments (B) into a shared-memory stage of
-//     an 8-deep ring in the canonical no-swizzle K-major layout, then split their own elements in
-//     place into TF32 high parts plus a remainder buffer;
+//     a register ring (the couplings are L2-resident; every load reads a valid clamped address and
+//     the values past the block are zeroed at split time, so nothing waits on a load early), split
+//     chunk c into TF32 high parts and rounded remainders and write them into a tensor-memory
+//     stage with tcgen05.st. The MMAs take this operand (A) straight from tensor memory;
+//   * moment warps (4-6): cp.async each chunk's source moments into a raw shared-memory ring (the
+//     permuted source rows of a symmetry-reduced pair are fetched a chunk ahead), then write them
+//     as the B operand, TF32 high parts plus remainders, in the canonical no-swizzle K-major layout;
 //   * one MMA thread (warp 11): per 8-wide k step the products hi*hi + hi*lo + lo*hi (the lo*lo
-//     term is below FP32 rounding) into an FP32 accumulator in tensor memory; commits release the
-//     operand stages;
+//     term is below FP32 rounding), N = 64 columns each, into an FP32 accumulator in tensor memory;
+//     one commit per chunk releases both operand stages. A tcgen05.mma costs its issuing thread
+//     about 50 cycles whatever its N (measured), so products are made as wide as the block allows;
 //   * drain warps (7-10, one per tensor-memory lane quarter): the tensor cores round each
-//     accumulation toward zero, so one FP32
-//     accumulator over a whole interaction list loses ~1e-4; accumulators live for 8 chunks only,
-//     two alternate, and each finished one is added into an FP64 sum in tensor memory, which the
-//     epilogue rounds once into the FP32 moments.
+//     accumulation toward zero, so one FP32 accumulator over a whole interaction list loses ~1e-4;
+//     accumulators live for 8 chunks only, two alternate, and each finished one is added into an
+//     FP64 sum in tensor memory, which the epilogue rounds once into the FP32 moments.
 //
-// Complex maps run as real GEMMs without expanding the moments: with a = op(B)[i, k] and the
-// moments interleaved (re, im) along k as they lie in memory,
-//   Re l = sum_k [ar, -ai] . [mr, mi],   Im l = sum_k [ai, ar] . [mr, mi],
-// so the coupling warps write two A operands (A_re = (ar, -ai), A_im = (ai, ar) per k) and every
-// B chunk feeds both accumulators. Adjoint maps conjugate a; symmetry-reduced couplings apply
-// their row / column permutations in the load addresses.
+// Complex maps run as real GEMMs: with B = Br + i Bi and m = mr + i mi,
+//   [Re l | Im l] = [Br Bi] (interleaved along k) x [[mr, mi]; [-mi, mr]] (interleaved rows),
+// so the coupling's interleaved (re, im) storage is the A operand as it lies in memory and each
+// moment value feeds two B rows (Re rows (mr, -mi), Im rows (mi, mr)). Adjoint maps conjugate B;
+// symmetry-reduced couplings apply their row / column permutations in the load addresses.
 //
 // Every wait on an mbarrier is bounded: a wait that gives up counts itself in a device counter
 // (h2b_tensor_wait_timeouts) and sets the CTA's abort flag; every role then leaves its loop, the
@@ -44,24 +44,35 @@ namespace h2b {
 namespace {
 
 constexpr int UM_M = 128;         // output rows per tile = tensor-memory lanes
-constexpr int UM_KC = 16;         // FP32 K values per chunk: 4 groups of 16 bytes per B row
+constexpr int UM_KC = 32;         // FP32 K values per chunk: 8 groups of 16 bytes per B row
 constexpr int UM_KG = UM_KC / 4;
-constexpr int UM_NA = 4;          // coupling stages in tensor memory
-constexpr int UM_NB = 8;          // moment stages in shared memory
-constexpr int UM_LAG = UM_NB - 2; // moment copies issued this many chunks ahead of the split
-constexpr int UM_SEG = 8;         // chunks per accumulation segment
+constexpr int UM_NS = 4;          // operand stages: coupling in tensor memory, moments in shared memory
+constexpr int UM_LAG = 4;         // moment copies issued this many chunks ahead of their expansion
+constexpr int UM_RS = UM_LAG + 2; // raw moment stages (a slot is rewritten two barriers after its last read)
+constexpr uint32_t UM_RAWROW = UM_KC * 4 + 16;  // raw moment row: one chunk's values + 16 bytes of padding
+// chunks per accumulation segment: 64 values of K are summed in FP32 (the tensor cores' own
+// rounding) before the segment is added to the FP64 sum (measured on the 65,536-point sphere:
+// relative error 3.4e-7 at 64 values, 6.5e-7 at 128, 1.2e-6 at 256; time +1 % per halving)
+constexpr int UM_SEG = 64 / UM_KC;
+// Every hand-off between the roles costs a fixed few hundred cycles whatever the chunk holds
+// (measured: with the products removed the kernel ran almost as fast as with them; 32-wide chunks
+// ran 27 % faster than 16-wide ones), so chunks are as wide as the tensor-memory and shared-memory
+// stages allow.
+constexpr int UM_AR = 4;          // coupling column stages in shared memory (bulk-copy path)
+constexpr int UM_ALA = 3;         // coupling columns copied this many chunks ahead
 // 4 coupling, 3 moment, 4 drain, 1 MMA: twelve warps place three on each SM sub-partition, whose
 // 16K registers then allow up to 170 per thread (a thirteenth warp would cap them at 128)
 constexpr int UM_WARPS = 12;
 constexpr int UM_BW = 3;           // moment warps
 constexpr int UM_BT = UM_BW * 32;  // moment threads
 constexpr int UM_THREADS = UM_WARPS * 32;
-constexpr int UM_NT_MAX_REAL = 64;    // MMA N (right-hand sides) per tile, real maps
-constexpr int UM_NT_MAX_CPLX = 32;    // complex maps (two accumulators: Re and Im)
+constexpr int UM_NT_MAX_REAL = 64;    // right-hand sides per tile, real maps (MMA N = 64)
+constexpr int UM_NT_MAX_CPLX = 32;    // complex maps: Re and Im rows make MMA N = 64
 constexpr uint32_t UM_LBO = 128;            // bytes between the two 16-byte K halves of a k step
 constexpr uint32_t UM_SBO = UM_KG * 128;    // bytes between 8-row groups (4 groups of 128 bytes)
-constexpr unsigned UM_SPIN = 1u << 22;      // default try_wait attempts before a wait gives up
-constexpr unsigned UM_SPIN_FINAL = 1u << 26;  // the final wait for products already issued
+constexpr unsigned UM_SUSPEND_NS = 1000;   // suspend-time hint of one try_wait attempt
+constexpr unsigned UM_SPIN = 1u << 20;      // default attempts before a wait gives up (about a second)
+constexpr unsigned UM_SPIN_FINAL = 1u << 23;  // the final wait for products already issued
 
 __device__ unsigned int g_umma_timeouts = 0;
 __device__ unsigned int g_umma_wait_limit = UM_SPIN;
@@ -125,22 +136,35 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(bar)), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+
+// bulk copy global -> this CTA's shared memory, completing `bytes` of the barrier's transaction count
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(su32(bar))
+                 : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(bar)) : "memory");
 }
 
 // bounded wait for the completion of the mbarrier phase with the given parity; false when it gave
-// up (counted in g_umma_timeouts)
+// up (counted in g_umma_timeouts). Each attempt suspends the thread until the phase completes or
+// UM_SUSPEND_NS pass, so waiting warps leave the issue slots to the warps that work beside them on
+// the same SM sub-partition (a spinning wait measured 2-3x slower producers).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned limit) {
     const uint32_t a = su32(bar);
     for (unsigned it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.b32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
-            : "r"(a), "r"(parity)
+            : "r"(a), "r"(parity), "n"(UM_SUSPEND_NS)
             : "memory");
         if (done) return true;
     }
@@ -156,6 +180,20 @@ __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, unsign
 }
 
 __device__ __forceinline__ bool warp_aborted(volatile int *flag) { return __any_sync(0xffffffffu, *flag != 0); }
+
+// named barrier 1 over the moment warps with an OR vote: every participant gets the same answer
+__device__ __forceinline__ bool bar_vote_or(bool v) {
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "barrier.cta.red.or.pred q, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(out)
+        : "r"((uint32_t)v), "n"(UM_BT)
+        : "memory");
+    return out != 0;
+}
 
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
     asm volatile(
@@ -196,6 +234,28 @@ template <int N> __device__ __forceinline__ void cp_wait_group() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// One chunk of a tile row (UM_KC FP32 values; complex: (re, im) of op(B)[row, k] along k' = 2k,
+// 2k + 1, conjugated for adjoint maps) split into TF32 high parts and remainders and written to the
+// row's tensor-memory lane: hi at columns [ta, ta + UM_KC), lo after them. Values past the block
+// (element index >= kv) are zero.
+template <int W>
+__device__ __forceinline__ void store_split(uint32_t ta, const float (&v)[UM_KC], int kv, bool adj) {
+#pragma unroll
+    for (int h = 0; h < UM_KC / 16; ++h) {
+        uint32_t hi[16], lo[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            const int j = 16 * h + e;
+            float x = (j / W) < kv ? v[j] : 0.0f;
+            if (W == 2 && adj && (j & 1)) x = -x;
+            split2(x, hi[e], lo[e]);
+        }
+        tmem_st16(ta + 16u * h, hi);
+        tmem_st16(ta + UM_KC + 16u * h, lo);
+    }
+    tmem_wait_st();
+}
+
 template <class T> struct UmScalar;
 template <> struct UmScalar<float> {
     static constexpr int W = 1;  // FP32 values per element
@@ -212,8 +272,9 @@ struct UmPair {
     const T *X;         // source moments of the tile's first right-hand side, column-major snc x nq
     int snc;            // source coefficients
     int nk;             // K chunks
-    const int *rowmap;  // output row -> row (forward) / column (transposed) of B, or null
-    const int *xmap;    // k -> source moment row, or null
+    const int *rowmap;  // output row -> row of the (forward or transposed) stored block, or null
+    const int *kmap;    // k -> column of the (forward or transposed) stored block, or null
+    bool vec;           // the moment columns start on 16-byte boundaries: whole 16-byte copies
 };
 
 template <class T>
@@ -223,20 +284,24 @@ __device__ __forceinline__ UmPair<T> um_pair(const DMap &m, const DSide &r, cons
     UmPair<T> u;
     u.snc = um_ncoef(t, t.level[r.i2o_src[p]]);
     u.nk = (W * u.snc + UM_KC - 1) / UM_KC;
-    u.B = static_cast<const T *>(m.cpl) + r.pair_cpl[p];
+    // transposed and adjoint products read the transposed copy: column kmap[k] of the stored block
+    u.B = static_cast<const T *>(fwd ? m.cpl : m.cpl_t) + r.pair_cpl[p];
     u.X = am + r.pair_src[p] * nrhs + (int64_t)q0 * u.snc;
     const int64_t ps = r.pair_perm ? r.pair_perm[p] : -1;
     u.rowmap = nullptr;
-    u.xmap = nullptr;
+    u.kmap = nullptr;
+    // both permutations act on the stored block, so the moments are read in their own order:
     if (ps >= 0) {
-        if (fwd) {  // t[rp[i], cp[j]] = M[i, j]: out[i] += sum_j M[rp^-1[i], j] x[cp[j]]
+        if (fwd) {  // t[rp[i], cp[j]] = M[i, j]: out[i] += sum_j M[rp^-1[i], cp^-1[j]] x[j]
             u.rowmap = m.perm + ps + nc;
-            u.xmap = m.perm + ps + 2 * nc;
-        } else {    // out[j] += sum_i op(M)[cp^-1[j], i] x[rp[i]]
+            u.kmap = m.perm + ps + 3 * u.snc;
+        } else {    // out[j] += sum_i op(M)[cp^-1[j], rp^-1[i]] x[i]
             u.rowmap = m.perm + ps + 3 * u.snc;
-            u.xmap = m.perm + ps;
+            u.kmap = m.perm + ps + u.snc;
         }
     }
+    constexpr int V = 16 / (int)sizeof(T);  // elements per 16 bytes
+    u.vec = (r.pair_src[p] * nrhs + (int64_t)q0 * u.snc) % V == 0 && u.snc % V == 0;
     return u;
 }
 
@@ -249,9 +314,10 @@ __global__ void __maxnreg__(168)
 i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mode, int nrhs, int qt_max,
                 const T *__restrict__ am, T *__restrict__ dm) {
     constexpr int W = UmScalar<T>::W;
+    constexpr int EB = sizeof(T);        // bytes per element (4 real, 8 complex)
     constexpr int KQ = UM_KC / W;        // elements along k per chunk
     extern __shared__ __align__(128) unsigned char um_smem[];
-    __shared__ uint64_t a_full[UM_NA], a_empty[UM_NA], b_full[UM_NB], b_empty[UM_NB];
+    __shared__ uint64_t a_full[UM_NS], b_full[UM_NS], empty[UM_NS], ar_full[UM_AR], ar_empty[UM_AR];
     __shared__ uint64_t acc_full[2], acc_empty[2], fin;
     __shared__ uint32_t tmem_slot;
     __shared__ int nchunks_s;
@@ -265,7 +331,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     if (m0 >= nc || q0 >= nq) return;  // whole CTA, before any barrier
     const int mt = min(UM_M, nc - m0);
     const int qt = min(qt_max, nq - q0);
-    const int np = ((qt_max + 15) / 16) * 16;      // MMA N of every tile (zero rows past qt)
+    const int np = ((W * qt_max + 15) / 16) * 16;   // MMA N: B rows (real: q; complex: Re rows, then Im rows)
     const int p0 = r.i2o_ptr[node], p1 = r.i2o_ptr[node + 1];
     T *out = dm + r.mom_off[node] * nrhs;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -276,13 +342,11 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     const bool fwd = mode == H2B_FORWARD, adj = mode == H2B_ADJOINT;
     const unsigned limit = g_umma_wait_limit;
 
-    // tensor memory: two accumulators of W * np columns (segments alternate between them), the
-    // FP64 sum (two columns per value), then UM_NA coupling stages of 32 * W columns (hi, lo)
-    const uint32_t acc_cols = (uint32_t)(W * np);
-    const uint32_t col_master = 2 * acc_cols;
-    const uint32_t col_a = 4 * acc_cols;
-    const uint32_t a_stage_cols = 32u * W;
-    const uint32_t need = col_a + UM_NA * a_stage_cols;
+    // tensor memory: two FP32 accumulators of np columns (segments alternate between them), the
+    // FP64 sum (two columns per value), then UM_NS coupling stages of 2 UM_KC columns (hi, lo)
+    const uint32_t col_master = 2 * (uint32_t)np;
+    const uint32_t col_a = 4 * (uint32_t)np;
+    const uint32_t need = col_a + UM_NS * 2 * UM_KC;
     const uint32_t ncols = need <= 64 ? 64u : (need <= 128 ? 128u : (need <= 256 ? 256u : 512u));
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_slot)),
@@ -291,17 +355,18 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int s = 0; s < UM_NA; ++s) {
+        for (int s = 0; s < UM_NS; ++s) {
             mbar_init(&a_full[s], 128);
-            mbar_init(&a_empty[s], 1);
-        }
-        for (int s = 0; s < UM_NB; ++s) {
             mbar_init(&b_full[s], UM_BT);
-            mbar_init(&b_empty[s], 1);
+            mbar_init(&empty[s], 1);
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
             mbar_init(&acc_empty[a], 128);
+        }
+        for (int a = 0; a < UM_AR; ++a) {
+            mbar_init(&ar_full[a], 1);
+            mbar_init(&ar_empty[a], 128);
         }
         mbar_init(&fin, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -320,39 +385,139 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     }
     const int C = nchunks_s;
     const int G = (C + UM_SEG - 1) / UM_SEG;
-    const uint32_t b_stage_bytes = 2u * (uint32_t)np * (UM_KC * 4);  // hi then lo
     const uint32_t smem0 = su32(um_smem);
+    const uint32_t b_stage_bytes = 2u * (uint32_t)np * (UM_KC * 4);  // hi then lo, canonical layout
+    const uint32_t raw0 = smem0 + UM_NS * b_stage_bytes;
+    const uint32_t raw_stage_bytes = (uint32_t)qt_max * UM_RAWROW;
+    const uint32_t acol_bytes = (uint32_t)nc * EB;                 // one stored coupling column
+    const uint32_t astage_bytes = ((uint32_t)KQ * acol_bytes + 127u) & ~127u;
+    const uint32_t araw0 = raw0 + ((UM_RS * raw_stage_bytes + 127u) & ~127u);
 
-    if (warp < 4) {
+    if (warp < 4 && m.cpl_vec) {
+        // ---------------- coupling warps, bulk-copy path ----------------
+        // Per chunk, lane j of warp 0 copies column kmap[k0 + j] of the pair's stored block (nc
+        // contiguous values) into a shared-memory stage with a bulk copy, UM_ALA chunks ahead; every
+        // thread then reads its own row of those columns, so the scattered accesses of a permuted
+        // block stay in shared memory and global memory is read in whole columns.
+        const int row = 32 * warp + lane;   // tile row = tensor-memory lane
+        const bool live = row < mt;
+        const uint32_t tl = tmem + ((uint32_t)(32 * warp) << 16);
+        int lp = p0, lk = 0;  // consumption cursor
+        UmPair<T> lu = um_pair<T>(m, r, t, p0, nc, fwd, nrhs, q0, am);
+        int brow = live ? (lu.rowmap ? lu.rowmap[m0 + row] : m0 + row) : 0;
+        int ip = p0, ik = 0, ic = 0;  // copy cursor (warp 0)
+        UmPair<T> iu = lu;
+        int kcol = 0;  // lane j: stored column of the copy chunk's k = ik KQ + j
+        auto fetch_col = [&]() {
+            const int k = min(ik * KQ + lane, iu.snc - 1);
+            kcol = iu.kmap ? __ldg(iu.kmap + k) : k;
+        };
+        auto issue = [&]() -> bool {  // warp 0: the columns of chunk ic
+            const int st = ic % UM_AR;
+            if (ic >= UM_AR && !warp_wait(&ar_empty[st], ((ic / UM_AR) - 1) & 1, limit)) return false;
+            const int nv = min(KQ, iu.snc - ik * KQ);
+            const uint32_t dst = araw0 + (uint32_t)st * astage_bytes;
+            if (lane == 0) mbar_expect_tx(&ar_full[st], (uint32_t)nv * acol_bytes);
+            __syncwarp();
+            if (lane < nv) bulk_copy(dst + (uint32_t)lane * acol_bytes, iu.B + (int64_t)kcol * nc, acol_bytes, &ar_full[st]);
+            __syncwarp();
+            ++ic;
+            if (++ik == iu.nk) {
+                ik = 0;
+                if (++ip < p1) iu = um_pair<T>(m, r, t, ip, nc, fwd, nrhs, q0, am);
+            }
+            if (ip < p1) fetch_col();
+            return true;
+        };
+        int cw = 0;  // chunks whose columns this warp has waited for
+        if (warp == 0) {
+            fetch_col();
+            for (int u = 0; u < UM_ALA && ic < C; ++u)
+                if (!issue()) abort_s = 1;
+        }
+        for (int c = 0; c < C; ++c) {
+            if (warp_aborted(&abort_s)) break;
+            if (warp == 0 && ic < C && !issue()) {
+                abort_s = 1;
+                break;
+            }
+            const int st = c % UM_AR;
+            if (!warp_wait(&ar_full[st], (c / UM_AR) & 1, limit)) {
+                abort_s = 1;
+                break;
+            }
+            const int kv = live ? min(KQ, lu.snc - lk * KQ) : 0;
+            const uint32_t src = araw0 + (uint32_t)st * astage_bytes + (uint32_t)brow * EB;
+            float v[UM_KC];
+#pragma unroll
+            for (int j = 0; j < KQ; ++j) {
+                if constexpr (W == 2) {
+                    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
+                                 : "=f"(v[2 * j]), "=f"(v[2 * j + 1])
+                                 : "r"(src + (uint32_t)j * acol_bytes));
+                } else {
+                    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v[j]) : "r"(src + (uint32_t)j * acol_bytes));
+                }
+            }
+            mbar_arrive(&ar_empty[st]);
+            if (++lk == lu.nk) {
+                lk = 0;
+                if (++lp < p1) {
+                    lu = um_pair<T>(m, r, t, lp, nc, fwd, nrhs, q0, am);
+                    brow = live ? (lu.rowmap ? lu.rowmap[m0 + row] : m0 + row) : 0;
+                }
+            }
+            const int s = c % UM_NS;
+            if (c >= UM_NS && !warp_wait(&empty[s], ((c / UM_NS) - 1) & 1, limit)) {
+                abort_s = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t ta = tl + col_a + (uint32_t)s * (2u * UM_KC);
+            store_split<W>(ta, v, kv, adj);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(&a_full[s]);
+            cw = c + 1;
+        }
+        if (warp == 0) {
+            // bulk copies issued but not consumed (after a wait gave up) still write this CTA's
+            // shared memory: wait for them, with the full bound, before the CTA can exit
+            for (int cc = cw; cc < ic; ++cc) mbar_wait(&ar_full[cc % UM_AR], (cc / UM_AR) & 1, UM_SPIN_FINAL);
+        }
+    } else if (warp < 4) {
         // ---------------- coupling warps: A operand into tensor memory ----------------
         const int row = 32 * warp + lane;   // tile row = tensor-memory lane
         const bool live = row < mt;
         const uint32_t tl = tmem + ((uint32_t)(32 * warp) << 16);
-        // load cursor: pair lp, chunk lk, the pair's operands and this thread's row of B
+        // load cursor: pair lp, chunk lk, the pair's operands and this thread's row of op(B), one
+        // chunk ahead; every load reads a valid address (clamped row and k) and the values past the
+        // block are zeroed when the chunk is split, so no instruction waits on a load early
         int lp = p0, lk = 0;
         UmPair<T> lu = um_pair<T>(m, r, t, p0, nc, fwd, nrhs, q0, am);
         int brow = live ? (lu.rowmap ? lu.rowmap[m0 + row] : m0 + row) : 0;
-        float ra[4][UM_KC];
-        auto load = [&](float (&v)[UM_KC]) {
-            const int k0 = lk * KQ;
-            if constexpr (W == 2) {
+        float ra[2][UM_KC];
+        int kv[2];    // valid elements of each buffered chunk (0 for rows past the tile)
+        int km[KQ];   // stored-block indices of the next chunk's k (its permutation, fetched a chunk ahead)
+        auto fetch_map = [&]() {
 #pragma unroll
-                for (int j = 0; j < KQ; ++j) {
-                    const int k = k0 + j;
-                    float2 x = make_float2(0.f, 0.f);
-                    if (live && k < lu.snc)
-                        x = fwd ? ldg2(lu.B + brow + (int64_t)k * nc) : ldg2(lu.B + k + (int64_t)brow * lu.snc);
+            for (int j = 0; j < KQ; ++j) {
+                const int k = min(lk * KQ + j, lu.snc - 1);
+                km[j] = lu.kmap ? __ldg(lu.kmap + k) : k;
+            }
+        };
+        auto load = [&](float (&v)[UM_KC], int &nvalid) {
+            const int k0 = lk * KQ;
+            nvalid = live ? min(KQ, lu.snc - k0) : 0;
+#pragma unroll
+            for (int j = 0; j < KQ; ++j) {
+                const int k = km[j];
+                const T *src = lu.B + brow + (int64_t)k * nc;
+                if constexpr (W == 2) {
+                    const float2 x = ldg2(src);
                     v[2 * j] = x.x;
                     v[2 * j + 1] = x.y;
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < KQ; ++j) {
-                    const int k = k0 + j;
-                    float x = 0.f;
-                    if (live && k < lu.snc)
-                        x = fwd ? __ldg(lu.B + brow + (int64_t)k * nc) : __ldg(lu.B + k + (int64_t)brow * lu.snc);
-                    v[j] = x;
+                } else {
+                    v[j] = __ldg(src);
                 }
             }
             if (++lk == lu.nk) {
@@ -362,49 +527,24 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
                     brow = live ? (lu.rowmap ? lu.rowmap[m0 + row] : m0 + row) : 0;
                 }
             }
+            if (lp < p1) fetch_map();
         };
+        fetch_map();
+        load(ra[0], kv[0]);
+        for (int c0 = 0; c0 < C; c0 += 2) {
 #pragma unroll
-        for (int u = 0; u < 3; ++u)
-            if (u < C) load(ra[u]);
-        for (int c0 = 0; c0 < C; c0 += 4) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 2; ++u) {
                 const int c = c0 + u;
                 if (c >= C || warp_aborted(&abort_s)) break;
-                if (c + 3 < C) load(ra[(u + 3) & 3]);
-                const int s = c % UM_NA;
-                if (c >= UM_NA && !warp_wait(&a_empty[s], ((c / UM_NA) - 1) & 1, limit)) {
+                if (c + 1 < C) load(ra[u ^ 1], kv[u ^ 1]);
+                const int s = c % UM_NS;
+                if (c >= UM_NS && !warp_wait(&empty[s], ((c / UM_NS) - 1) & 1, limit)) {
                     abort_s = 1;
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t ta = tl + col_a + (uint32_t)s * a_stage_cols;
-                uint32_t hi[16], lo[16];
-                if constexpr (W == 2) {
-                    // A_re = (ar, -ai), A_im = (ai, ar) per complex k; a = conj(B) for adjoint maps
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const float ar = ra[u][2 * j], ai = adj ? -ra[u][2 * j + 1] : ra[u][2 * j + 1];
-                        split2(ar, hi[2 * j], lo[2 * j]);
-                        split2(-ai, hi[2 * j + 1], lo[2 * j + 1]);
-                    }
-                    tmem_st16(ta, hi);
-                    tmem_st16(ta + 16, lo);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const float ar = ra[u][2 * j], ai = adj ? -ra[u][2 * j + 1] : ra[u][2 * j + 1];
-                        split2(ai, hi[2 * j], lo[2 * j]);
-                        split2(ar, hi[2 * j + 1], lo[2 * j + 1]);
-                    }
-                    tmem_st16(ta + 32, hi);
-                    tmem_st16(ta + 48, lo);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) split2(ra[u][j], hi[j], lo[j]);
-                    tmem_st16(ta, hi);
-                    tmem_st16(ta + 16, lo);
-                }
-                tmem_wait_st();
+                const uint32_t ta = tl + col_a + (uint32_t)s * (2u * UM_KC);
+                store_split<W>(ta, ra[u], kv[u], adj);
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 mbar_arrive(&a_full[s]);
             }
@@ -413,23 +553,27 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     } else if (warp < 4 + UM_BW) {
         // ---------------- moment warps: B operand into shared memory ----------------
         const int bt = tid - 128;
-        // this thread's 16-byte pieces (row q, k group kg) of every chunk: pieces bt, bt + UM_BT, ...
-        const int npieces = np * UM_KG;
-        int cp_ = p0, ck = 0;  // copy cursor
+        // copy cursor (pair cp_, chunk ck); a chunk's raw moments are qt_max rows of 64 bytes, copied
+        // as 16-byte pieces (consecutive threads: consecutive pieces of a row), element by element
+        // where a column is not 16-byte aligned or the chunk runs past the pair's coefficients
+        int cp_ = p0, ck = 0;
         UmPair<T> cu = um_pair<T>(m, r, t, p0, nc, fwd, nrhs, q0, am);
-        auto issue = [&](int c) {
-            const uint32_t hb = smem0 + (uint32_t)(c % UM_NB) * b_stage_bytes;
+        constexpr int EV = 16 / EB;  // elements per piece
+        auto issue = [&](int ci) {
+            const uint32_t rb = raw0 + (uint32_t)(ci % UM_RS) * raw_stage_bytes;
             const int k0 = ck * KQ;
-            for (int pc = bt; pc < npieces; pc += UM_BT) {
-                const int q = pc >> 2, kg = pc & 3;
-                const uint32_t dst = hb + goff(q, kg);
+            for (int pc = bt; pc < qt_max * UM_KG; pc += UM_BT) {
+                const int q = pc / UM_KG, kg = pc % UM_KG, kp = k0 + kg * EV;
+                const uint32_t dst = rb + (uint32_t)q * UM_RAWROW + (uint32_t)kg * 16;
+                const T *src = cu.X + (int64_t)q * cu.snc + kp;
+                if (cu.vec && q < qt && kp + EV <= cu.snc) {
+                    cp_elem<16>(dst, src, true);
+                } else {
 #pragma unroll
-                for (int e = 0; e < 4 / W; ++e) {
-                    const int k = k0 + kg * (4 / W) + e;
-                    const bool ok = q < qt && k < cu.snc;
-                    const T *src = cu.X;
-                    if (ok) src = cu.X + (int64_t)q * cu.snc + (cu.xmap ? __ldg(cu.xmap + k) : k);
-                    cp_elem<sizeof(T)>(dst + (uint32_t)(e * sizeof(T)), src, ok);
+                    for (int e = 0; e < EV; ++e) {
+                        const bool ok = q < qt && kp + e < cu.snc;
+                        cp_elem<EB>(dst + (uint32_t)(e * EB), ok ? src + e : cu.X, ok);
+                    }
                 }
             }
             if (++ck == cu.nk) {
@@ -441,35 +585,62 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             issue(c);
             cp_commit_group();
         }
+        const int npieces = np * UM_KG;  // 16-byte pieces of the expanded tile
+        const int rr0 = bt % np, kg0 = bt / np;
         for (int c = 0; c < C; ++c) {
             const int ci = c + UM_LAG;
-            if (ci < C) {
-                // stage ci % UM_NB was last read by the products of chunk ci - UM_NB
-                if (ci >= UM_NB && !mbar_wait(&b_empty[ci % UM_NB], ((ci / UM_NB) - 1) & 1, limit)) abort_s = 1;
-                if (abort_s) break;
-                issue(ci);
-            }
+            if (ci < C) issue(ci);
             cp_commit_group();
             cp_wait_group<UM_LAG>();  // this thread's copies of chunk c have landed
-            const uint32_t hb = smem0 + (uint32_t)(c % UM_NB) * b_stage_bytes;
+            // ... and everyone's; the vote makes the stop decision the same for all moment threads
+            // (a thread that left the loop alone would leave the others waiting at this barrier)
+            if (bar_vote_or(abort_s != 0)) break;
+            const int s = c % UM_NS;
+            // the expanded stage was last read by the products of chunk c - UM_NS
+            if (c >= UM_NS && !mbar_wait(&empty[s], ((c / UM_NS) - 1) & 1, limit)) {
+                abort_s = 1;  // the stage may still be read: leave it; the next vote stops the loop
+                continue;
+            }
+            const uint32_t rb = raw0 + (uint32_t)(c % UM_RS) * raw_stage_bytes;
+            const uint32_t hb = smem0 + (uint32_t)s * b_stage_bytes;
             const uint32_t lb = hb + (uint32_t)np * (UM_KC * 4);
+            // pieces bt, bt + UM_BT, ... as (row rr, k group kg), rows fastest: a quarter-warp writes
+            // 8 consecutive rows of one k group (conflict-free); stepped without a division
+            int rr = rr0, kg = kg0;
             for (int pc = bt; pc < npieces; pc += UM_BT) {
-                const uint32_t o = goff(pc >> 2, pc & 3);
-                float v[4];
-                asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                             : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
-                             : "r"(hb + o));
+                if (pc != bt) {
+                    rr += UM_BT;
+                    while (rr >= np) {
+                        rr -= np;
+                        ++kg;
+                    }
+                }
+                float v[4] = {0.f, 0.f, 0.f, 0.f};
+                if (W == 1 ? rr < qt_max : rr < 2 * qt_max) {
+                    const int q = W == 1 ? rr : (rr < qt_max ? rr : rr - qt_max);
+                    float w[4];
+                    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                                 : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3])
+                                 : "r"(rb + (uint32_t)q * UM_RAWROW + (uint32_t)kg * 16));
+                    if (W == 1) {
+                        v[0] = w[0], v[1] = w[1], v[2] = w[2], v[3] = w[3];
+                    } else if (rr < qt_max) {  // Re rows: (mr, -mi) per k
+                        v[0] = w[0], v[1] = -w[1], v[2] = w[2], v[3] = -w[3];
+                    } else {                   // Im rows: (mi, mr) per k
+                        v[0] = w[1], v[1] = w[0], v[2] = w[3], v[3] = w[2];
+                    }
+                }
                 uint32_t h[4], l[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) split2(v[e], h[e], l[e]);
+                const uint32_t o = goff(rr, kg);
                 asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(hb + o), "r"(h[0]), "r"(h[1]), "r"(h[2]),
                              "r"(h[3]));
                 asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(lb + o), "r"(l[0]), "r"(l[1]), "r"(l[2]),
                              "r"(l[3]));
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(&b_full[c % UM_NB]);
-            if (abort_s) break;
+            mbar_arrive(&b_full[s]);
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
     } else if (warp < UM_WARPS - 1) {
@@ -490,19 +661,25 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            for (uint32_t j = 0; j < acc_cols; j += 8) {
-                uint32_t f[8], w[16];
-                tmem_ld8(tl + (uint32_t)a * acc_cols + j, f);
-                if (g > 0) tmem_ld16(tl + col_master + 2 * j, w);
+            for (int j = 0; j < np; j += 16) {
+                uint32_t f[16], w0[16], w1[16];
+                tmem_ld16(tl + (uint32_t)(a * np + j), f);
+                if (g > 0) {
+                    tmem_ld16(tl + col_master + 2u * (uint32_t)j, w0);
+                    tmem_ld16(tl + col_master + 2u * (uint32_t)j + 16u, w1);
+                }
                 tmem_wait_ld();
 #pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    const double prev = g > 0 ? __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]) : 0.0;
+                for (int e = 0; e < 16; ++e) {
+                    uint32_t &lo = e < 8 ? w0[2 * e] : w1[2 * (e - 8)];
+                    uint32_t &hi = e < 8 ? w0[2 * e + 1] : w1[2 * (e - 8) + 1];
+                    const double prev = g > 0 ? __hiloint2double((int)hi, (int)lo) : 0.0;
                     const double v = prev + (double)__uint_as_float(f[e]);
-                    w[2 * e] = (uint32_t)__double2loint(v);
-                    w[2 * e + 1] = (uint32_t)__double2hiint(v);
+                    lo = (uint32_t)__double2loint(v);
+                    hi = (uint32_t)__double2hiint(v);
                 }
-                tmem_st16(tl + col_master + 2 * j, w);
+                tmem_st16(tl + col_master + 2u * (uint32_t)j, w0);
+                tmem_st16(tl + col_master + 2u * (uint32_t)j + 16u, w1);
             }
             tmem_wait_st();
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -513,7 +690,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             for (int j8 = 0; j8 * 8 < qt; ++j8) {
                 uint32_t wr[16], wi[16];
                 tmem_ld16(tl + col_master + 2 * (uint32_t)(8 * j8), wr);
-                if constexpr (W == 2) tmem_ld16(tl + col_master + 2 * (uint32_t)(np + 8 * j8), wi);
+                if constexpr (W == 2) tmem_ld16(tl + col_master + 2 * (uint32_t)(qt_max + 8 * j8), wi);
                 tmem_wait_ld();
                 if (row < mt) {
 #pragma unroll
@@ -533,38 +710,28 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             }
         }
     } else if (lane == 0) {
-        // ---------------- MMA thread ----------------
+        // ---------------- MMA thread: six products of N = np columns per chunk ----------------
         const uint32_t idesc = tf32_idesc(UM_M, np);
-        const uint32_t b_hi0 = smem0;
-        int c = 0;
-        for (; c < C; ++c) {
-            const int sa = c % UM_NA, sb = c % UM_NB, g = c / UM_SEG, a = g & 1;
+        for (int c = 0; c < C; ++c) {
+            const int s = c % UM_NS, g = c / UM_SEG, a = g & 1;
             if (c % UM_SEG == 0 && g >= 2 && !mbar_wait(&acc_empty[a], ((g >> 1) - 1) & 1, limit)) abort_s = 1;
-            if (!abort_s && !mbar_wait(&a_full[sa], (c / UM_NA) & 1, limit)) abort_s = 1;
-            if (!abort_s && !mbar_wait(&b_full[sb], (c / UM_NB) & 1, limit)) abort_s = 1;
+            if (!abort_s && !mbar_wait(&a_full[s], (c / UM_NS) & 1, limit)) abort_s = 1;
+            if (!abort_s && !mbar_wait(&b_full[s], (c / UM_NS) & 1, limit)) abort_s = 1;
             if (abort_s) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t dre = tmem + (uint32_t)a * acc_cols;
-            const uint32_t ta = tmem + col_a + (uint32_t)sa * a_stage_cols;
-            const uint32_t bh = b_hi0 + (uint32_t)sb * b_stage_bytes, bl = bh + (uint32_t)np * (UM_KC * 4);
+            const uint32_t d = tmem + (uint32_t)(a * np);
+            const uint32_t ta = tmem + col_a + (uint32_t)s * (2u * UM_KC);
+            const uint32_t bh = smem0 + (uint32_t)s * b_stage_bytes, bl = bh + (uint32_t)np * (UM_KC * 4);
 #pragma unroll
             for (int j = 0; j < UM_KC / 8; ++j) {
                 const uint64_t dbh = kmajor_desc(bh + (uint32_t)j * 2 * UM_LBO);
                 const uint64_t dbl = kmajor_desc(bl + (uint32_t)j * 2 * UM_LBO);
                 const uint32_t first = (c % UM_SEG != 0 || j > 0) ? 1u : 0u;
-                const uint32_t ah = ta + 8u * j, al = ah + 16u;
-                umma_ts(dre, ah, dbh, idesc, first);
-                umma_ts(dre, ah, dbl, idesc, 1u);
-                umma_ts(dre, al, dbh, idesc, 1u);
-                if constexpr (W == 2) {
-                    const uint32_t dim = dre + (uint32_t)np;
-                    umma_ts(dim, ah + 32u, dbh, idesc, first);
-                    umma_ts(dim, ah + 32u, dbl, idesc, 1u);
-                    umma_ts(dim, al + 32u, dbh, idesc, 1u);
-                }
+                umma_ts(d, ta + 8u * j, dbh, idesc, first);
+                umma_ts(d, ta + 8u * j, dbl, idesc, 1u);
+                umma_ts(d, ta + UM_KC + 8u * j, dbh, idesc, 1u);
             }
-            umma_commit(&a_empty[sa]);
-            umma_commit(&b_empty[sb]);
+            umma_commit(&empty[s]);
             if (c % UM_SEG == UM_SEG - 1 || c == C - 1) umma_commit(&acc_full[a]);
         }
     }
@@ -596,14 +763,31 @@ cudaError_t launch_i2o_umma(bool cplx, const DMap &m, const DSide &recv, const D
     const int ntmax = cplx ? UM_NT_MAX_CPLX : UM_NT_MAX_REAL;
     // right-hand sides per tile: at most ntmax, tiles of equal width
     const int ntiles = (nq + ntmax - 1) / ntmax;
-    const int qt_max = (nq + ntiles - 1) / ntiles;
-    const int np = ((qt_max + 15) / 16) * 16;
-    const size_t smem = (size_t)UM_NB * 2 * np * UM_KC * 4;  // moment stages (hi and lo)
+    // a multiple of 8, so that the imaginary rows of a complex tile start on a 16-column boundary
+    // of tensor memory; rows past the right-hand sides are zero
+    const int qt_max = ((nq + ntiles - 1) / ntiles + 7) / 8 * 8;
+    const int np = (((cplx ? 2 : 1) * qt_max + 15) / 16) * 16;
+    // expanded moment stages (hi and lo), the raw moment ring and the coupling column stages
+    const size_t eb = cplx ? 8 : 4, kq = cplx ? UM_KC / 2 : UM_KC;
+    const size_t raw = ((size_t)UM_RS * qt_max * UM_RAWROW + 127) & ~(size_t)127;
+    const size_t acols = (size_t)UM_AR * ((kq * maxcoef * eb + 127) & ~(size_t)127);
+    size_t smem = (size_t)UM_NS * 2 * np * UM_KC * 4 + raw;
+    // the coupling column stages grow with the block size; blocks whose stages do not fit beside
+    // the moment stages are read by the register path instead
+    int dev = 0, optin = 0;
+    cudaError_t e0 = cudaGetDevice(&dev);
+    if (e0 == cudaSuccess) e0 = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e0 != cudaSuccess) return e0;
+    DMap mm = m;
+    if (mm.cpl_vec && smem + acols + 1024 <= (size_t)optin)
+        smem += acols;
+    else
+        mm.cpl_vec = 0;
     const dim3 grid(nnodes, (maxcoef + UM_M - 1) / UM_M, ntiles);
     auto go = [&](auto kern, auto *am, auto *dm) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        kern<<<grid, UM_THREADS, smem, st>>>(m, recv, src, nodes, fa.mode, fa.nrhs, qt_max, am, dm);
+        kern<<<grid, UM_THREADS, smem, st>>>(mm, recv, src, nodes, fa.mode, fa.nrhs, qt_max, am, dm);
         return cudaGetLastError();
     };
     if (cplx)

@@ -153,13 +153,23 @@ class MatvecServer:
                     r = self._admit(key)
                 except AdmissionError as exc:
                     while q:
-                        q.popleft().future.set_exception(exc)
+                        f = q.popleft().future
+                        if f.set_running_or_notify_cancel():
+                            f.set_exception(exc)
                     break
                 free = [s for s in r.slots if not getattr(s, "busy", False)]
                 if not free:
                     break
                 slot = free[0]
-                block = [q.popleft() for _ in range(min(self.max_block, len(q)))]
+                block = []
+                while q and len(block) < self.max_block:
+                    req = q.popleft()
+                    # a request its client cancelled before it started is dropped here; once in a
+                    # block it can no longer be cancelled
+                    if req.future.set_running_or_notify_cancel():
+                        block.append(req)
+                if not block:
+                    continue
                 slot.busy = True
                 r.busy += 1
                 r.last_used = time.perf_counter()
@@ -181,7 +191,8 @@ class MatvecServer:
                 for req, y in zip(t.requests, ys):
                     req.t_done = now
                     self.latencies.append(now - req.t_submit)
-                    req.future.set_result(y)
+                    if not req.future.done():
+                        req.future.set_result(y)
                 t.slot.busy = False
                 t.resident.busy -= 1
                 done_any = True
@@ -344,3 +355,54 @@ class DenseExecutor:
 
     def results(self, slot, ticket, k):
         return [ticket["Y"][:, i] for i in range(k)]
+
+
+# ---------------------------------------------------------------------------------------------
+# Replicas: maps partitioned over devices
+# ---------------------------------------------------------------------------------------------
+class ReplicaRouter:
+    """Serve many maps on several devices, one server per device, no collective on the data path.
+
+    A single map's product does not shard (each level's I2O needs the moments of all boxes), but
+    the serving workload -- many independent maps and requests -- does: each map is assigned to
+    one device when it is added (the device with the fewest bytes assigned so far, by its server's
+    footprint estimate), and its requests go to that device's server. `servers` are MatvecServer
+    objects, typically one per GPU (GpuExecutor(device)); with one process per GPU, each process
+    builds a router over its own device and the maps it owns.
+    """
+
+    def __init__(self, servers):
+        self.servers = list(servers)
+        if not self.servers:
+            raise ValueError("at least one server")
+        self.device_of = {}
+        self.assigned = [0] * len(self.servers)
+
+    def add_map(self, key, description) -> int:
+        """Register a map on the least-loaded device; returns that device's index."""
+        if key in self.device_of:
+            raise KeyError(f"map {key!r} already added")
+        sizes = []
+        for d, srv in enumerate(self.servers):
+            need = srv.executor.footprint(description, srv.max_block, srv.nslots)
+            sizes.append((self.assigned[d] + need, d, need))
+        _, d, need = min(sizes)
+        self.servers[d].add_map(key, description)
+        self.device_of[key] = d
+        self.assigned[d] += need
+        return d
+
+    def submit(self, key, x, mode="forward"):
+        return self.servers[self.device_of[key]].submit(key, x, mode)
+
+    def stats(self) -> dict:
+        per = [s.stats() for s in self.servers]
+        lat = np.concatenate([np.asarray(s.latencies) for s in self.servers if s.latencies]) \
+            if any(s.latencies for s in self.servers) else np.zeros(1)
+        return {"devices": per, "requests": int(sum(p["requests"] for p in per)),
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "assigned_bytes": list(self.assigned)}
+
+    def close(self) -> None:
+        for s in self.servers:
+            s.close()

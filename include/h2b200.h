@@ -223,8 +223,9 @@ const char *h2b_last_error(void);
  * No counterpart in the reference: its CPU map has no device-side waits. */
 h2b_status h2b_tensor_wait_timeouts(int32_t device, uint32_t *count);
 
-/* Bound of every mbarrier wait of the tensor-core kernels on `device`, in try_wait attempts; 0
- * restores the default (2^22). A low bound makes the waits give up, which is how tests exercise
+/* Bound of every mbarrier wait of the tensor-core kernels on `device`, in try_wait attempts of at
+ * most a microsecond each; 0 restores the default (2^20, about a second). A low bound makes the
+ * waits give up, which is how tests exercise
  * the timeout path without faulting or hanging anything: the kernels then stop, wait for the
  * products they issued, free their tensor memory and return, and h2b_matvec_host reports
  * H2B_ERR_CUDA. Waits for the device's queued work. No counterpart in the reference. */

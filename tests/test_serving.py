@@ -108,3 +108,90 @@ def test_unknown_map_is_rejected():
     with pytest.raises(KeyError):
         srv.submit("missing", np.ones(3))
     srv.close()
+
+
+def test_cancelled_requests_are_dropped_and_the_server_survives():
+    """A client may cancel a request it no longer needs (an iterative solver that converged): a
+    request cancelled before its block starts is dropped, the others are answered, and the
+    scheduler keeps running."""
+    rng = np.random.default_rng(5)
+    (A,) = mats(rng, [30])
+    srv = MatvecServer(DenseExecutor(delay=0.05), budget_bytes=1e9, max_block=4, slots=1)
+    srv.add_map("a", A)
+    xs = [rng.standard_normal(30) for _ in range(20)]
+    futs = [srv.submit("a", x) for x in xs]
+    cancelled = [f.cancel() for f in futs[8:16]]  # those still queued behind the first blocks
+    assert any(cancelled)
+    for x, f, c in zip(xs, futs, [False] * 8 + cancelled + [False] * 4):
+        if c:
+            assert f.cancelled()
+        else:
+            assert np.allclose(f.result(timeout=10), A @ x)
+    assert np.allclose(srv.submit("a", xs[0]).result(timeout=10), A @ xs[0])  # still serving
+    srv.close()
+
+
+def test_a_client_that_dies_mid_stream_does_not_stop_the_others():
+    """Clients are independent threads; one that dies after submitting (it never collects its
+    result) leaves the server and the other clients' requests unaffected."""
+    rng = np.random.default_rng(6)
+    (A,) = mats(rng, [25])
+    srv = MatvecServer(DenseExecutor(delay=0.002), budget_bytes=1e9, max_block=8, slots=2)
+    srv.add_map("a", A)
+    errors, done = [], []
+
+    def client(i, die):
+        r = np.random.default_rng(100 + i)
+        for j in range(15):
+            x = r.standard_normal(25)
+            f = srv.submit("a", x, ("forward", "transpose", "adjoint")[j % 3])
+            if die and j == 5:
+                raise RuntimeError("client crashed")  # dies with a request in flight
+            op = (A, A.T, A.conj().T)[j % 3]
+            if not np.allclose(f.result(timeout=10), op @ x):
+                errors.append((i, j))
+        done.append(i)
+
+    def run(i, die):
+        try:
+            client(i, die)
+        except RuntimeError:
+            pass
+
+    ts = [threading.Thread(target=run, args=(i, i == 3)) for i in range(8)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=30)
+    assert not errors and sorted(done) == [0, 1, 2, 4, 5, 6, 7]
+    st = srv.stats()
+    srv.close()
+    assert st["requests"] >= 7 * 15 + 6  # the dead client's submitted requests were answered too
+
+
+def test_replica_router_balances_maps_and_routes_requests():
+    from h2factory_b200.serving import ReplicaRouter
+
+    rng = np.random.default_rng(7)
+    sizes = [40, 30, 40, 20, 30, 50]
+    maps = mats(rng, sizes)
+    exs = [DenseExecutor() for _ in range(3)]
+    router = ReplicaRouter([MatvecServer(e, budget_bytes=1e9, max_block=4, slots=1) for e in exs])
+    devs, load = [], [0, 0, 0]
+    for i, M in enumerate(maps):
+        need = exs[0].footprint(M, 4, 1)
+        d = router.add_map(f"m{i}", M)
+        assert load[d] == min(load)  # each map goes to the least-loaded device at its arrival
+        load[d] += need
+        devs.append(d)
+    assert sorted(set(devs)) == [0, 1, 2] and router.assigned == load
+    for i, M in enumerate(maps):
+        x = rng.standard_normal(M.shape[0])
+        assert np.allclose(router.submit(f"m{i}", x, "adjoint").result(timeout=10), M.conj().T @ x)
+    st = router.stats()
+    router.close()
+    assert st["requests"] == len(maps)
+    # each map was loaded by its own device only
+    assert sum(e.loads for e in exs) == len(maps)
+    for d, e in enumerate(exs):
+        assert e.loads == devs.count(d)
