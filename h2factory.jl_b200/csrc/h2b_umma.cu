@@ -59,6 +59,7 @@ constexpr int UM_SEG = 64 / UM_KC;
 // ran 27 % faster than 16-wide ones), so chunks are as wide as the tensor-memory and shared-memory
 // stages allow.
 constexpr int UM_AR = 4;          // coupling column stages in shared memory (bulk-copy path)
+constexpr int UM_AI = 4;          // warps that issue a chunk's column copies (KQ / UM_AI columns each)
 constexpr int UM_ALA = 3;         // coupling columns copied this many chunks ahead
 // 4 coupling, 3 moment, 4 drain, 1 MMA: twelve warps place three on each SM sub-partition, whose
 // 16K registers then allow up to 170 per thread (a thirteenth warp would cap them at 128)
@@ -317,7 +318,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
     constexpr int EB = sizeof(T);        // bytes per element (4 real, 8 complex)
     constexpr int KQ = UM_KC / W;        // elements along k per chunk
     extern __shared__ __align__(128) unsigned char um_smem[];
-    __shared__ uint64_t a_full[UM_NS], b_full[UM_NS], empty[UM_NS], ar_full[UM_AR], ar_empty[UM_AR];
+    __shared__ uint64_t a_full[UM_NS], b_full[UM_NS], empty[UM_NS], ar_full[UM_AI][UM_AR], ar_empty[UM_AR];
     __shared__ uint64_t acc_full[2], acc_empty[2], fin;
     __shared__ uint32_t tmem_slot;
     __shared__ int nchunks_s;
@@ -365,7 +366,7 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             mbar_init(&acc_empty[a], 128);
         }
         for (int a = 0; a < UM_AR; ++a) {
-            mbar_init(&ar_full[a], 1);
+            for (int w = 0; w < UM_AI; ++w) mbar_init(&ar_full[w][a], 1);
             mbar_init(&ar_empty[a], 128);
         }
         mbar_init(&fin, 1);
@@ -395,8 +396,9 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
 
     if (warp < 4 && m.cpl_vec) {
         // ---------------- coupling warps, bulk-copy path ----------------
-        // Per chunk, lane j of warp 0 copies column kmap[k0 + j] of the pair's stored block (nc
-        // contiguous values) into a shared-memory stage with a bulk copy, UM_ALA chunks ahead; every
+        // Per chunk, lane j of issuing warp w copies column kmap[k0 + w KQ / UM_AI + j] of the pair's
+        // stored block (nc contiguous values) into a shared-memory stage with a bulk copy, UM_ALA
+        // chunks ahead (each issuing warp completes its own barrier of the stage); every
         // thread then reads its own row of those columns, so the scattered accesses of a permuted
         // block stay in shared memory and global memory is read in whole columns.
         const int row = 32 * warp + lane;   // tile row = tensor-memory lane
@@ -405,21 +407,25 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
         int lp = p0, lk = 0;  // consumption cursor
         UmPair<T> lu = um_pair<T>(m, r, t, p0, nc, fwd, nrhs, q0, am);
         int brow = live ? (lu.rowmap ? lu.rowmap[m0 + row] : m0 + row) : 0;
-        int ip = p0, ik = 0, ic = 0;  // copy cursor (warp 0)
+        int ip = p0, ik = 0, ic = 0;  // copy cursor (issuing warps)
         UmPair<T> iu = lu;
-        int kcol = 0;  // lane j: stored column of the copy chunk's k = ik KQ + j
+        constexpr int JW = KQ / UM_AI;  // columns copied by each issuing warp
+        const int jw = warp * JW;       // this warp's first column of a chunk
+        const bool issuer = warp < UM_AI;
+        int kcol = 0;  // lane j: stored column of the copy chunk's k = ik KQ + jw + j
         auto fetch_col = [&]() {
-            const int k = min(ik * KQ + lane, iu.snc - 1);
+            const int k = min(ik * KQ + jw + lane, iu.snc - 1);
             kcol = iu.kmap ? __ldg(iu.kmap + k) : k;
         };
-        auto issue = [&]() -> bool {  // warp 0: the columns of chunk ic
+        auto issue = [&]() -> bool {  // issuing warp: its columns of chunk ic
             const int st = ic % UM_AR;
             if (ic >= UM_AR && !warp_wait(&ar_empty[st], ((ic / UM_AR) - 1) & 1, limit)) return false;
-            const int nv = min(KQ, iu.snc - ik * KQ);
-            const uint32_t dst = araw0 + (uint32_t)st * astage_bytes;
-            if (lane == 0) mbar_expect_tx(&ar_full[st], (uint32_t)nv * acol_bytes);
+            const int nv = max(0, min(JW, iu.snc - ik * KQ - jw));
+            const uint32_t dst = araw0 + (uint32_t)st * astage_bytes + (uint32_t)jw * acol_bytes;
+            if (lane == 0) mbar_expect_tx(&ar_full[warp][st], (uint32_t)nv * acol_bytes);
             __syncwarp();
-            if (lane < nv) bulk_copy(dst + (uint32_t)lane * acol_bytes, iu.B + (int64_t)kcol * nc, acol_bytes, &ar_full[st]);
+            if (lane < nv)
+                bulk_copy(dst + (uint32_t)lane * acol_bytes, iu.B + (int64_t)kcol * nc, acol_bytes, &ar_full[warp][st]);
             __syncwarp();
             ++ic;
             if (++ik == iu.nk) {
@@ -430,19 +436,22 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             return true;
         };
         int cw = 0;  // chunks whose columns this warp has waited for
-        if (warp == 0) {
+        if (issuer) {
             fetch_col();
             for (int u = 0; u < UM_ALA && ic < C; ++u)
                 if (!issue()) abort_s = 1;
         }
         for (int c = 0; c < C; ++c) {
             if (warp_aborted(&abort_s)) break;
-            if (warp == 0 && ic < C && !issue()) {
+            if (issuer && ic < C && !issue()) {
                 abort_s = 1;
                 break;
             }
             const int st = c % UM_AR;
-            if (!warp_wait(&ar_full[st], (c / UM_AR) & 1, limit)) {
+            bool landed = true;
+#pragma unroll
+            for (int w = 0; w < UM_AI; ++w) landed = landed && warp_wait(&ar_full[w][st], (c / UM_AR) & 1, limit);
+            if (!landed) {
                 abort_s = 1;
                 break;
             }
@@ -479,10 +488,10 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             mbar_arrive(&a_full[s]);
             cw = c + 1;
         }
-        if (warp == 0) {
+        if (issuer) {
             // bulk copies issued but not consumed (after a wait gave up) still write this CTA's
-            // shared memory: wait for them, with the full bound, before the CTA can exit
-            for (int cc = cw; cc < ic; ++cc) mbar_wait(&ar_full[cc % UM_AR], (cc / UM_AR) & 1, UM_SPIN_FINAL);
+            // shared memory: wait for this warp's, with the full bound, before the CTA can exit
+            for (int cc = cw; cc < ic; ++cc) mbar_wait(&ar_full[warp][cc % UM_AR], (cc / UM_AR) & 1, UM_SPIN_FINAL);
         }
     } else if (warp < 4) {
         // ---------------- coupling warps: A operand into tensor memory ----------------
@@ -585,8 +594,17 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             issue(c);
             cp_commit_group();
         }
-        const int npieces = np * UM_KG;  // 16-byte pieces of the expanded tile
-        const int rr0 = bt % np, kg0 = bt / np;
+        // rows past the right-hand sides' rows (real tiles whose width is not a multiple of 16)
+        // are zero in every stage, written once
+        for (int o = bt; o < UM_NS * 2 * (np - W * qt_max) * UM_KG; o += UM_BT) {
+            const int rr = W * qt_max + (o / UM_KG) % (np - W * qt_max), kg = o % UM_KG;
+            const int sh = o / (UM_KG * (np - W * qt_max));  // stage and hi/lo half
+            asm volatile("st.shared.v4.b32 [%0], {%1, %1, %1, %1};" ::"r"(smem0 + (uint32_t)sh * ((uint32_t)np * UM_KC * 4) +
+                                                                         goff(rr, kg)),
+                         "r"(0u));
+        }
+        const int npieces = qt_max * UM_KG;  // 16-byte pieces of the raw tile
+        const int q0p = bt % qt_max, kg0 = bt / qt_max;
         for (int c = 0; c < C; ++c) {
             const int ci = c + UM_LAG;
             if (ci < C) issue(ci);
@@ -604,40 +622,44 @@ i2o_umma_kernel(DMap m, DSide r, DSide t, const int *__restrict__ nodes, int mod
             const uint32_t rb = raw0 + (uint32_t)(c % UM_RS) * raw_stage_bytes;
             const uint32_t hb = smem0 + (uint32_t)s * b_stage_bytes;
             const uint32_t lb = hb + (uint32_t)np * (UM_KC * 4);
-            // pieces bt, bt + UM_BT, ... as (row rr, k group kg), rows fastest: a quarter-warp writes
-            // 8 consecutive rows of one k group (conflict-free); stepped without a division
-            int rr = rr0, kg = kg0;
+            // raw pieces bt, bt + UM_BT, ... as (row q, k group kg), rows fastest: a quarter-warp
+            // reads 8 rows of one k group and writes 8 consecutive rows of the expanded tile
+            // (conflict-free); a complex piece (mr, mi) of two k is split once and written to
+            // both its rows, Re (mr, -mi) and Im (mi, mr): negation is exact in TF32 parts
+            int q = q0p, kg = kg0;
             for (int pc = bt; pc < npieces; pc += UM_BT) {
                 if (pc != bt) {
-                    rr += UM_BT;
-                    while (rr >= np) {
-                        rr -= np;
+                    q += UM_BT;
+                    while (q >= qt_max) {
+                        q -= qt_max;
                         ++kg;
                     }
                 }
-                float v[4] = {0.f, 0.f, 0.f, 0.f};
-                if (W == 1 ? rr < qt_max : rr < 2 * qt_max) {
-                    const int q = W == 1 ? rr : (rr < qt_max ? rr : rr - qt_max);
-                    float w[4];
-                    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-                                 : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3])
-                                 : "r"(rb + (uint32_t)q * UM_RAWROW + (uint32_t)kg * 16));
-                    if (W == 1) {
-                        v[0] = w[0], v[1] = w[1], v[2] = w[2], v[3] = w[3];
-                    } else if (rr < qt_max) {  // Re rows: (mr, -mi) per k
-                        v[0] = w[0], v[1] = -w[1], v[2] = w[2], v[3] = -w[3];
-                    } else {                   // Im rows: (mi, mr) per k
-                        v[0] = w[1], v[1] = w[0], v[2] = w[3], v[3] = w[2];
-                    }
-                }
+                float w[4];
+                asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                             : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3])
+                             : "r"(rb + (uint32_t)q * UM_RAWROW + (uint32_t)kg * 16));
                 uint32_t h[4], l[4];
 #pragma unroll
-                for (int e = 0; e < 4; ++e) split2(v[e], h[e], l[e]);
-                const uint32_t o = goff(rr, kg);
-                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(hb + o), "r"(h[0]), "r"(h[1]), "r"(h[2]),
-                             "r"(h[3]));
-                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(lb + o), "r"(l[0]), "r"(l[1]), "r"(l[2]),
-                             "r"(l[3]));
+                for (int e = 0; e < 4; ++e) split2(w[e], h[e], l[e]);
+                const uint32_t o = goff(q, kg);
+                if constexpr (W == 1) {
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(hb + o), "r"(h[0]), "r"(h[1]),
+                                 "r"(h[2]), "r"(h[3]));
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(lb + o), "r"(l[0]), "r"(l[1]),
+                                 "r"(l[2]), "r"(l[3]));
+                } else {
+                    constexpr uint32_t S = 0x80000000u;
+                    const uint32_t oi = goff(qt_max + q, kg);
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(hb + o), "r"(h[0]), "r"(h[1] ^ S),
+                                 "r"(h[2]), "r"(h[3] ^ S));
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(lb + o), "r"(l[0]), "r"(l[1] ^ S),
+                                 "r"(l[2]), "r"(l[3] ^ S));
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(hb + oi), "r"(h[1]), "r"(h[0]),
+                                 "r"(h[3]), "r"(h[2]));
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(lb + oi), "r"(l[1]), "r"(l[0]),
+                                 "r"(l[3]), "r"(l[2]));
+                }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(&b_full[s]);
