@@ -7,6 +7,8 @@ stream into multi-RHS products:
 
 * requests on the same (map, orientation) that are waiting when a slot frees up are coalesced into
   one block of up to `max_block` right-hand sides (one matvec reads the near blocks once for all);
+  a request carries one right-hand side (a vector) or several (an n x k matrix, k <= max_block),
+  and a block holds whole requests;
 * every map has `slots` workspaces, each on its own CUDA stream, so blocks of different maps and
   orientations -- and consecutive blocks of one map -- run concurrently on the device; requests
   that arrive while blocks are in flight are admitted as soon as a slot is free (continuous
@@ -42,6 +44,7 @@ class Request:
     future: Future
     t_submit: float
     t_done: float = 0.0
+    ncols: int = 1          # right-hand sides carried (1 for a vector)
 
 
 @dataclass
@@ -94,11 +97,16 @@ class MatvecServer:
             self.maps[key] = description
 
     def submit(self, key, x, mode: str | int = "forward") -> Future:
-        """Queue y = op(A_key) x; the future resolves to y (numpy)."""
+        """Queue y = op(A_key) x for a vector x or an n x k block of right-hand sides (k <=
+        max_block); the future resolves to y of the same shape (numpy, or a CUDA tensor for a
+        CUDA x)."""
         m = MODES[mode] if isinstance(mode, str) else int(mode)
         fut = Future()
         xv = x if getattr(x, "is_cuda", False) else np.asarray(x)  # device tensors stay on the device
-        req = Request(key, m, xv, fut, time.perf_counter())
+        k = 1 if xv.ndim == 1 else int(xv.shape[1])
+        if xv.ndim > 2 or not 1 <= k <= self.max_block:
+            raise ValueError(f"a request carries 1 to {self.max_block} right-hand sides, got shape {tuple(xv.shape)}")
+        req = Request(key, m, xv, fut, time.perf_counter(), ncols=k)
         with self._lock:
             if key not in self.maps:
                 raise KeyError(key)
@@ -161,13 +169,14 @@ class MatvecServer:
                 if not free:
                     break
                 slot = free[0]
-                block = []
-                while q and len(block) < self.max_block:
+                block, cols = [], 0
+                while q and cols + q[0].ncols <= self.max_block:
                     req = q.popleft()
                     # a request its client cancelled before it started is dropped here; once in a
                     # block it can no longer be cancelled
                     if req.future.set_running_or_notify_cancel():
                         block.append(req)
+                        cols += req.ncols
                 if not block:
                     continue
                 slot.busy = True
@@ -175,7 +184,7 @@ class MatvecServer:
                 r.last_used = time.perf_counter()
                 handle = self.executor.launch(slot, mode, [b.x for b in block])
                 self.inflight.append(_Ticket(r, slot, block, handle))
-                self.blocks.append(len(block))
+                self.blocks.append(cols)
                 launched = True
             if not q:
                 del self.pending[(key, mode)]
@@ -186,7 +195,7 @@ class MatvecServer:
         keep = []
         for t in self.inflight:
             if self.executor.done(t.handle):
-                ys = self.executor.results(t.slot, t.handle, len(t.requests))
+                ys = self.executor.results(t.slot, t.handle, [req.x.ndim == 2 and req.ncols for req in t.requests])
                 now = time.perf_counter()
                 for req, y in zip(t.requests, ys):
                     req.t_done = now
@@ -288,24 +297,33 @@ class GpuExecutor:
         from .core import OrientedMap, mul_
 
         torch = self.torch
-        k = len(xs)
+        widths = [1 if xi.ndim == 1 else int(xi.shape[1]) for xi in xs]
+        k = sum(widths)
         core = slot.ws.core
         nin = core.size[1] if mode == 0 else core.size[0]
         nout = core.size[0] if mode == 0 else core.size[1]
         on_device = getattr(xs[0], "is_cuda", False)
         with torch.cuda.stream(slot.stream):
             if on_device:
-                for i, xi in enumerate(xs):
-                    slot.x[i, :nin].copy_(xi, non_blocking=True)
+                c = 0
+                for xi, w in zip(xs, widths):
+                    # rows of slot.x are right-hand sides: a block's columns become rows
+                    slot.x[c:c + w, :nin].copy_(xi.reshape(nin, w).t(), non_blocking=True)
+                    c += w
             else:
-                host = torch.from_numpy(np.ascontiguousarray(np.stack(xs, axis=0)))
+                rows = [np.asarray(xi).reshape(nin, w).T for xi, w in zip(xs, widths)]
+                host = torch.from_numpy(np.ascontiguousarray(np.concatenate(rows, axis=0)))
                 slot.x[:k, :nin].copy_(host, non_blocking=False)
             X = slot.x[:k, :nin].t()
             Y = slot.y[:k, :nout].t()
             A = slot.ws if mode == 0 else OrientedMap(slot.ws, mode)
             mul_(Y, A, X, stream=slot.stream.cuda_stream)
             if on_device:
-                slot.out = [slot.y[i, :nout].clone() for i in range(k)]
+                out, c = [], 0
+                for xi, w in zip(xs, widths):
+                    out.append(slot.y[c, :nout].clone() if xi.ndim == 1 else slot.y[c:c + w, :nout].t().clone())
+                    c += w
+                slot.out = out
             else:
                 slot.out = slot.y[:k, :nout].to("cpu", non_blocking=True)
             slot.event.record(slot.stream)
@@ -314,11 +332,12 @@ class GpuExecutor:
     def done(self, event) -> bool:
         return event.query()
 
-    def results(self, slot, event, k):
+    def results(self, slot, event, shapes):
+        """The block's outputs per request; `shapes` holds False for a vector request and the
+        column count of a block request."""
         if isinstance(slot.out, list):
             return slot.out
-        y = slot.out.numpy()
-        return [y[i].copy() for i in range(k)]
+        return _split_rows(slot.out.numpy(), shapes)
 
 
 class DenseExecutor:
@@ -347,14 +366,27 @@ class DenseExecutor:
 
     def launch(self, slot, mode, xs):
         A = slot.mat if mode == 0 else (slot.mat.T if mode == 1 else slot.mat.conj().T)
-        X = np.stack(xs, axis=1)
+        X = np.concatenate([np.asarray(x).reshape(x.shape[0], -1) for x in xs], axis=1)
         return {"t": time.perf_counter() + self.delay, "Y": A @ X}
 
     def done(self, ticket) -> bool:
         return time.perf_counter() >= ticket["t"]
 
-    def results(self, slot, ticket, k):
-        return [ticket["Y"][:, i] for i in range(k)]
+    def results(self, slot, ticket, shapes):
+        return _split_rows(ticket["Y"].T, shapes)
+
+
+def _split_rows(rows, shapes):
+    """Rows of a block's output (one per right-hand side) back into per-request results."""
+    out, c = [], 0
+    for w in shapes:
+        if w:
+            out.append(np.ascontiguousarray(rows[c:c + w].T))
+            c += w
+        else:
+            out.append(rows[c].copy())
+            c += 1
+    return out
 
 
 # ---------------------------------------------------------------------------------------------

@@ -195,3 +195,30 @@ def test_replica_router_balances_maps_and_routes_requests():
     assert sum(e.loads for e in exs) == len(maps)
     for d, e in enumerate(exs):
         assert e.loads == devs.count(d)
+
+
+def test_block_requests_mixed_with_vectors():
+    """Requests of 1 and k right-hand sides share blocks; a block never exceeds max_block columns,
+    every result has its request's shape, and a request wider than max_block is refused."""
+    rng = np.random.default_rng(8)
+    (A,) = mats(rng, [36])
+    srv = MatvecServer(DenseExecutor(delay=0.005), budget_bytes=1e9, max_block=8, slots=1)
+    srv.add_map("a", A)
+    subs = []
+    for i in range(40):
+        k = (1, 3, 8, 1, 5)[i % 5]
+        x = rng.standard_normal((36, k)) + 1j * rng.standard_normal((36, k))
+        if k == 1 and i % 2:
+            x = x[:, 0]
+        mode = ("forward", "transpose", "adjoint")[i % 3]
+        subs.append((x, mode, srv.submit("a", x, mode)))
+    with pytest.raises(ValueError):
+        srv.submit("a", np.zeros((36, 9)))
+    for x, mode, f in subs:
+        op = {"forward": A, "transpose": A.T, "adjoint": A.conj().T}[mode]
+        y = f.result(timeout=10)
+        assert y.shape == x.shape
+        assert np.allclose(y, op @ x, rtol=1e-13, atol=1e-12)
+    srv.close()
+    assert max(srv.blocks) <= 8
+    assert sum(srv.blocks) == sum(1 if x.ndim == 1 else x.shape[1] for x, _, _ in subs)

@@ -1,7 +1,8 @@
 """Serving loop on the GPU: each result is the same alone and in the mix (GPU).
 
-Several client threads issue forward / transpose / adjoint requests on two resident maps; the
-server coalesces them into multi-RHS blocks on concurrent stream slots. Every result must equal
+Several client threads issue forward / transpose / adjoint requests of one or three right-hand
+sides on two resident maps; the server coalesces them into multi-RHS blocks on concurrent stream
+slots. Every result must equal
 the same product computed alone (one right-hand side, through h2b_matvec_host) to a relative
 1e-12 -- the blocked kernels sum each column in the same order as the single-column ones up to
 FP64 rounding.
@@ -48,9 +49,10 @@ def test_results_alone_and_in_the_mix(device_requests):
             core = maps[key]
             mode = int(r.integers(3))
             n = core.trial.npoints
-            x = r.standard_normal(n)
+            shape = (n, 3) if r.integers(3) == 0 else (n,)  # some requests carry 3 right-hand sides
+            x = r.standard_normal(shape)
             if core.field == "complex":
-                x = x + 1j * r.standard_normal(n)
+                x = x + 1j * r.standard_normal(shape)
             xs = torch.from_numpy(x).to("cuda:0") if device_requests else x
             if device_requests:
                 torch.cuda.synchronize()
@@ -69,6 +71,9 @@ def test_results_alone_and_in_the_mix(device_requests):
     srv.close()
     assert len(jobs) == 72
     assert st["mean_block"] >= 1.0
+    assert any(x.ndim == 2 for _, _, x, _ in jobs)
     for key, mode, x, y in jobs:
-        want = alone[key].matvec_host(x, mode)
-        assert np.linalg.norm(y - want) / np.linalg.norm(want) < 1e-12, (key, mode)
+        assert y.shape == x.shape
+        for xc, yc in zip(x.reshape(x.shape[0], -1).T, y.reshape(y.shape[0], -1).T):
+            want = alone[key].matvec_host(np.ascontiguousarray(xc), mode)
+            assert np.linalg.norm(yc - want) / np.linalg.norm(want) < 1e-12, (key, mode)
