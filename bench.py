@@ -713,7 +713,8 @@ def serve_arm(args):
         cores.append(core)
     build_s = time.perf_counter() - t_build
     max_block = 32
-    srv = MatvecServer(GpuExecutor(0), budget_bytes=150e9, max_block=max_block, slots=2)
+    srv = MatvecServer(GpuExecutor(0), budget_bytes=150e9, max_block=max_block, slots=2,
+                       max_inflight=args.serve_inflight or None)
     for i, c in enumerate(cores):
         srv.add_map(i, fp32_twin(c))
     rng = np.random.default_rng(31)
@@ -759,6 +760,7 @@ def serve_arm(args):
                    "clients": 256, "arrivals": "open-loop Poisson", "mode_mix": "60/20/20 forward/transpose/adjoint",
                    "rhs_per_request": widths, "rates_req_per_s": rates, "seconds_per_rate": args.serve_seconds,
                    "budget_bytes": 150e9, "max_block": max_block, "slots_per_map": 2,
+                   "max_inflight_blocks": args.serve_inflight or None,
                    "step": "one rate x request width for --serve-seconds",
                    "scale": "maps of --serve-n points (the configuration's generator draws 1,048,576)",
                    "build_s": round(build_s, 1)},
@@ -779,7 +781,7 @@ def _open_loop(srv, xs, nmaps, width, rate, seconds, rng):
     u = rng.random(arrivals.size)
     modes = np.where(u < 0.6, 0, np.where(u < 0.8, 1, 2))
     done_t = np.full(arrivals.size, np.nan)
-    futs = []
+    live = {}  # requests not yet answered (answered ones drop their results at once)
     srv.latencies.clear()
     srv.blocks.clear()
     lag = []
@@ -794,12 +796,19 @@ def _open_loop(srv, xs, nmaps, width, rate, seconds, rng):
                 pass
         lag.append(time.perf_counter() - t0 - ta)
         f = srv.submit(int(maps[i]), xs[(int(maps[i]), width)], int(modes[i]))
-        f.add_done_callback(lambda _f, i=i: _f.cancelled() or done_t.__setitem__(i, time.perf_counter() - t0))
-        futs.append(f)
+        live[i] = f
+
+        def answered(_f, i=i):
+            if not _f.cancelled():
+                done_t[i] = time.perf_counter() - t0
+            live.pop(i, None)
+
+        f.add_done_callback(answered)
     t_end = time.perf_counter() - t0
-    cancelled = sum(1 for f in futs if f.cancel())  # not started: dropped by the server
+    rest = list(live.values())
+    cancelled = sum(1 for f in rest if f.cancel())  # not started: dropped by the server
     deadline = time.perf_counter() + 120
-    for f in futs:
+    for f in rest:
         if not f.cancelled():
             f.result(timeout=max(1.0, deadline - time.perf_counter()))
     window = max(seconds, t_end)
@@ -924,6 +933,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="window per rate of the serving mode")
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000", help="request rates of the serving mode")
     ap.add_argument("--serve-rhs", default="1,8", help="right-hand sides per request of the serving mode")
+    ap.add_argument("--serve-inflight", type=int, default=4,
+                    help="blocks on the device at once in the serving mode (0: one per free slot of every map)")
     ap.add_argument("--batched", action="store_true",
                     help="time the batched-uneven configuration's shape (eager vs one graph replay per pass)")
     ap.add_argument("--maps", type=int, default=None, help="maps of the batched (96) or serving (32) mode")

@@ -13,6 +13,11 @@ stream into multi-RHS products:
   orientations -- and consecutive blocks of one map -- run concurrently on the device; requests
   that arrive while blocks are in flight are admitted as soon as a slot is free (continuous
   batching, not a queue drained one block at a time);
+* `max_inflight` caps the blocks on the device at once over all maps. With many resident maps an
+  uncapped server launches a narrow block per map and orientation, the device's launch queues
+  fill, and every block costs about as much as a full one (the dense M2L tiles 32 complex
+  right-hand sides); capped, the waiting requests of a (map, orientation) coalesce into wide
+  blocks, launched oldest request first;
 * a map is admitted only if its core and workspaces fit the budget; idle maps are evicted least
   recently used first, and reloaded from their host description on the next request.
 
@@ -72,8 +77,10 @@ class AdmissionError(MemoryError):
 class MatvecServer:
     """Serve matvec requests on resident maps with continuous batching."""
 
-    def __init__(self, executor, budget_bytes: float, max_block: int = 16, slots: int = 2):
+    def __init__(self, executor, budget_bytes: float, max_block: int = 16, slots: int = 2,
+                 max_inflight: int | None = None):
         self.executor = executor
+        self.max_inflight = max_inflight
         self.budget = float(budget_bytes)
         self.max_block = int(max_block)
         self.nslots = int(slots)
@@ -154,9 +161,14 @@ class MatvecServer:
 
     def _launch_ready(self) -> bool:
         launched = False
-        for (key, mode) in list(self.pending.keys()):
+        order = list(self.pending.keys())
+        if self.max_inflight is not None:
+            order.sort(key=lambda km: self.pending[km][0].t_submit if self.pending[km] else 0.0)
+        for (key, mode) in order:
             q = self.pending[(key, mode)]
             while q:
+                if self.max_inflight is not None and len(self.inflight) >= self.max_inflight:
+                    return launched
                 try:
                     r = self._admit(key)
                 except AdmissionError as exc:

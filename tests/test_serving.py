@@ -222,3 +222,42 @@ def test_block_requests_mixed_with_vectors():
     srv.close()
     assert max(srv.blocks) <= 8
     assert sum(srv.blocks) == sum(1 if x.ndim == 1 else x.shape[1] for x, _, _ in subs)
+
+
+def test_inflight_cap_coalesces_and_serves_oldest_first():
+    """With max_inflight blocks on the device at once, waiting requests coalesce into wider blocks
+    and the queue whose oldest request waited longest launches next."""
+    rng = np.random.default_rng(9)
+    maps = mats(rng, [30, 30, 30], cplx=False)
+
+    class Counting(DenseExecutor):
+        def __init__(self):
+            super().__init__(delay=0.01)
+            self.live, self.peak, self.order = 0, 0, []
+
+        def launch(self, slot, mode, xs):
+            self.live += 1
+            self.peak = max(self.peak, self.live)
+            self.order.append(next(i for i, M in enumerate(maps) if slot.mat is M))
+            return super().launch(slot, mode, xs)
+
+        def results(self, slot, ticket, shapes):
+            self.live -= 1
+            return super().results(slot, ticket, shapes)
+
+    ex = Counting()
+    srv = MatvecServer(ex, budget_bytes=1e9, max_block=16, slots=2, max_inflight=1)
+    for i, M in enumerate(maps):
+        srv.add_map(i, M)
+    subs = []
+    for j in range(60):
+        i = j % 3
+        x = rng.standard_normal(30)
+        subs.append((i, x, srv.submit(i, x)))
+    for i, x, f in subs:
+        assert np.allclose(f.result(timeout=20), maps[i] @ x)
+    srv.close()
+    assert ex.peak == 1
+    assert np.mean(srv.blocks) > 3  # requests waited behind the single block and coalesced
+    # round robin by age: no map waits for two launches of another while it has a request queued
+    assert all(ex.order[k] != ex.order[k + 1] for k in range(min(6, len(ex.order) - 1)))
