@@ -91,6 +91,7 @@ struct SideHost {
     int n_init_leaves = 0;
     int64_t npairs = 0;
     SibGroups sib;                      // Toeplitz I2O by sibling groups (ngroups = 0: per node)
+    GroupTiles grp;                     // dense I2O for few right-hand sides, grouped by stored block
     int maxslen = 1;
     std::vector<int64_t> mom_off_host;  // moment offsets per unit rhs (host copy)
     std::vector<int64_t> spec_off_host; // spectrum offsets per unit rhs (host copy)
@@ -477,6 +478,68 @@ h2b_status upload_far_scalars(h2b_core *c, const double *src, int64_t count, con
 
 h2b_status upload_list(h2b_core *c, const std::vector<int> &v, int **dst) {
     CUDA_TRY(c->upload(dst, v.data(), v.size()));
+    return H2B_OK;
+}
+
+// Chunks and tiles of the grouped dense I2O (GroupTiles) for the receiving nodes of side `s`:
+// chunks of up to GT_R consecutive receiving nodes of one level; per chunk, its pairs sorted by
+// stored block, then by their rank among the receiver's pairs reading that block, then by receiver,
+// and cut into tiles of at most GT_P pairs with one block and distinct receivers.
+h2b_status build_group_tiles(h2b_core *c, const h2b_side_desc &s, SideHost &h,
+                             const std::vector<int64_t> &cpl_elem_off) {
+    std::vector<int> recv;
+    for (int n = 0; n < s.nnodes; ++n)
+        if (s.i2o_ptr[n + 1] > s.i2o_ptr[n]) recv.push_back(n);
+    if (recv.empty()) return H2B_OK;
+    std::vector<int> chunk_ptr{0}, rcv, tile_ptr{0}, tile_pp{0}, pair;
+    std::vector<unsigned char> slot;
+    struct E { int64_t key; int rank, slot, p; };
+    size_t i = 0;
+    while (i < recv.size()) {
+        const int lvl = s.level[recv[i]];
+        const size_t j0 = i;
+        while (i < recv.size() && (int)(i - j0) < GT_R && s.level[recv[i]] == lvl) rcv.push_back(recv[i++]);
+        std::vector<E> es;
+        for (size_t j = j0; j < i; ++j) {
+            const int n = recv[j];
+            std::map<int64_t, int> rank;
+            for (int p = s.i2o_ptr[n]; p < s.i2o_ptr[n + 1]; ++p) {
+                const int64_t key = cpl_elem_off[p];
+                es.push_back({key, rank[key]++, (int)(j - j0), p});
+            }
+        }
+        std::sort(es.begin(), es.end(), [](const E &a, const E &b) {
+            return a.key != b.key ? a.key < b.key : (a.rank != b.rank ? a.rank < b.rank : a.slot < b.slot);
+        });
+        unsigned used = 0;
+        int64_t key = -1;
+        int len = 0;
+        for (const E &e : es) {
+            if (len > 0 && (e.key != key || len == GT_P || (used >> e.slot & 1u))) {
+                tile_pp.push_back((int)pair.size());
+                used = 0;
+                len = 0;
+            }
+            key = e.key;
+            used |= 1u << e.slot;
+            ++len;
+            pair.push_back(e.p);
+            slot.push_back((unsigned char)e.slot);
+        }
+        if (len > 0) tile_pp.push_back((int)pair.size());
+        chunk_ptr.push_back((int)rcv.size());
+        tile_ptr.push_back((int)tile_pp.size() - 1);
+    }
+    GroupTiles &g = h.grp;
+    int *q;
+    unsigned char *u;
+    CUDA_TRY(c->upload(&q, chunk_ptr.data(), chunk_ptr.size())); g.chunk_ptr = q;
+    CUDA_TRY(c->upload(&q, rcv.data(), rcv.size())); g.rcv = q;
+    CUDA_TRY(c->upload(&q, tile_ptr.data(), tile_ptr.size())); g.tile_ptr = q;
+    CUDA_TRY(c->upload(&q, tile_pp.data(), tile_pp.size())); g.tile_pp = q;
+    CUDA_TRY(c->upload(&q, pair.data(), pair.size())); g.pair = q;
+    CUDA_TRY(c->upload(&u, slot.data(), slot.size())); g.slot = u;
+    g.nchunks = (int)chunk_ptr.size() - 1;
     return H2B_OK;
 }
 
@@ -1044,6 +1107,9 @@ h2b_status build_core(h2b_core *c, const h2b_map_desc &d) {
         if (toep) {
             st = build_sibling_groups(c, sd, h, o.spec_off_host, off);
             if (st) return st;
+        } else if (d.coupling_kind == H2B_COUPLING_DENSE) {
+            st = build_group_tiles(c, sd, h, pcpl);
+            if (st) return st;
         }
     }
     return build_near(c, d);
@@ -1243,7 +1309,12 @@ h2b_status run_i2o(h2b_core *c, const SideHost &D, const SideHost &A, const FarA
         CUDA_TRY(launch_i2o_siblings(c->field == H2B_COMPLEX, c->precision, c->dmap, D.d, D.sib, D.maxslen, fa, st));
         return H2B_OK;
     }
-    CUDA_TRY(launch_i2o(c->field == H2B_COMPLEX, c->precision, c->dmap, D.d, A.d, D.d_recv, D.n_recv, fa,
+    const bool cplx = c->field == H2B_COMPLEX;
+    if (D.grp.nchunks > 0 && i2o_grouped_eligible(cplx, c->dmap, c->dmap.ncomp * fa.nrhs, maxcoef)) {
+        CUDA_TRY(launch_i2o_grouped(cplx, c->precision, c->dmap, D.d, A.d, D.grp, maxcoef, fa, st));
+        return H2B_OK;
+    }
+    CUDA_TRY(launch_i2o(cplx, c->precision, c->dmap, D.d, A.d, D.d_recv, D.n_recv, fa,
                         maxcoef, maxt, D.maxhalf, st));
     return H2B_OK;
 }

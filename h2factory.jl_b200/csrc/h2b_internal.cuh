@@ -156,6 +156,24 @@ struct SibGroups {
     const int *kof = nullptr;          // [nentries*8] coupling offset of (source, slot), -1 if no pair
 };
 
+// Dense I2O for few right-hand sides, grouped by stored block. The receiving nodes are cut into
+// chunks of at most GT_R nodes of one level; a chunk's pairs are listed in tiles, each tile a run of
+// pairs that read the same stored (canonical) coupling block, from distinct receiving nodes. One CTA
+// per chunk stages a block once per tile and applies it to all of the tile's pairs (the symmetry
+// permutations act on the gathered moments and on the output rows), summing into the chunk's
+// receiving nodes in shared memory: each pair's block is read once per tile instead of once per pair.
+constexpr int GT_R = 16;  // receiving nodes per chunk
+constexpr int GT_P = 16;  // pairs per tile
+struct GroupTiles {
+    int nchunks = 0;
+    const int *chunk_ptr = nullptr;      // [nchunks+1] into rcv
+    const int *rcv = nullptr;            // receiving nodes, chunk by chunk
+    const int *tile_ptr = nullptr;       // [nchunks+1] into tile_pp
+    const int *tile_pp = nullptr;        // [ntiles+1] into pair / slot
+    const int *pair = nullptr;           // pair index (into the side's pair arrays)
+    const unsigned char *slot = nullptr; // receiving node of the pair as its position in the chunk
+};
+
 // Per-call arguments of the far passes.
 struct FarArgs {
     int mode;     // H2B_FORWARD / H2B_TRANSPOSE / H2B_ADJOINT
@@ -198,6 +216,14 @@ cudaError_t copy_umma_timeouts_async(unsigned *host, cudaStream_t st);
 cudaError_t set_umma_wait_limit(unsigned limit);
 cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const DSide &recv,
                                 const SibGroups &g, int maxslen, const FarArgs &fa, cudaStream_t st);
+// The grouped dense I2O (GroupTiles) for W x nq <= GT_MAX_COLS field columns (W = 2 complex);
+// wider blocks take the tensor-core I2O (measured on a 65,536-point Laplace map, p = 6: grouped
+// 13 / 26 / 65 / 73 ms for 1-4 real right-hand sides against 98 / 150 / 152 ms for the per-node
+// tile kernel and 84 ms for the tcgen05 kernel from 4 columns on).
+constexpr int GT_MAX_COLS = 4;
+bool i2o_grouped_eligible(bool cplx, const DMap &m, int nq, int maxcoef);
+cudaError_t launch_i2o_grouped(bool cplx, int precision, const DMap &m, const DSide &recv, const DSide &src,
+                               const GroupTiles &gt, int maxcoef, const FarArgs &fa, cudaStream_t st);
 cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const DSide &s,
                                  const int *nodes, int nnodes, const uint8_t *received,
                                  const FarArgs &fa, int maxcoef, int maxsep, cudaStream_t st);

@@ -1138,6 +1138,153 @@ __global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, cons
 }
 
 // ---------------------------------------------------------------------------------------------
+// B1 for few right-hand sides, grouped by stored block (GroupTiles). One CTA per chunk of receiving
+// nodes of one level. For each tile (pairs reading one stored block, distinct receivers) the block
+// is staged in 64 x 32 pieces once for up to TG_Q columns (pairs x right-hand sides) and applied
+// on the FP64 tensor cores; each pair's symmetry permutation moves into the gather of its moments
+// (column permutation) and the row its products land on (row permutation), the canonical form of
+// symmetryreduceddense.jl:84-95. Products add into the chunk's sums in shared memory; the tiles
+// follow one another behind the tile product's block barriers, and within a tile every pair has
+// its own receiver, so no two threads add into one sum at once. The sums are written once at the
+// end (overwriting each receiving node's I2O output, as the per-node kernels do).
+// ---------------------------------------------------------------------------------------------
+// column blocks of TG_Q columns held at once per staged piece of a block (their FP64 fragments:
+// 4 doubles per block and lane for real sums, 8 for complex)
+template <class A> constexpr int gt_nb() { return sizeof(A) == 16 ? 4 : 8; }
+
+template <class T>
+__global__ void __launch_bounds__(256)
+i2o_grouped_kernel(DMap m, DSide r, DSide t, GroupTiles gt, int mode, int nrhs, const T *__restrict__ am,
+                   T *__restrict__ dm) {
+    using A = typename ScalarTraits<T>::Acc;
+    constexpr int GT_NB = gt_nb<A>();
+    extern __shared__ unsigned char smem_raw[];
+    A *Ms = reinterpret_cast<A *>(smem_raw), *Xs = Ms + TG_M * TG_LD, *Sum = Xs + GT_NB * TG_K * TG_Q;
+    // per pair of the current run (slot b * TG_Q + j: pair j of column block b): its moments' offset,
+    // its permutation set (-1: none) and its receiver's position in the chunk
+    __shared__ int64_t run_src[GT_NB * TG_Q], run_perm[GT_NB * TG_Q];
+    __shared__ int run_slot[GT_NB * TG_Q];
+    const int ch = blockIdx.x;
+    const int r0 = gt.chunk_ptr[ch], nr = gt.chunk_ptr[ch + 1] - r0;
+    const int nc = ncoef_of(r, r.level[gt.rcv[r0]]);
+    const int nq = m.ncomp * nrhs;
+    const bool fwd = mode == H2B_FORWARD, adj = mode == H2B_ADJOINT;
+    const T *B0 = static_cast<const T *>(m.cpl);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g4 = lane >> 2, t4 = lane & 3;
+    for (int o = threadIdx.x; o < nr * nq * nc; o += blockDim.x) Sum[o] = A{};
+    const int pq = TG_Q / nq;  // pairs per column block
+    const int t_end = gt.tile_ptr[ch + 1];
+    for (int tl = gt.tile_ptr[ch]; tl < t_end;) {
+        // a run of tiles reading one stored block, cut into column blocks of pq pairs (at most
+        // GT_NB): every block holds pairs of distinct receivers, since each tile does
+        const int pf = gt.pair[gt.tile_pp[tl]];
+        const int64_t key = r.pair_cpl[pf];
+        int bs[GT_NB], bn[GT_NB], nb = 0;  // first pair and pair count of each block
+        int tl2 = tl;
+        while (tl2 < t_end && r.pair_cpl[gt.pair[gt.tile_pp[tl2]]] == key) {
+            const int e0 = gt.tile_pp[tl2], e1 = gt.tile_pp[tl2 + 1];
+            const int need = (e1 - e0 + pq - 1) / pq;
+            if (nb + need > GT_NB) break;
+            for (int e = e0; e < e1; e += pq) {
+                bs[nb] = e;
+                bn[nb] = min(pq, e1 - e);
+                ++nb;
+            }
+            ++tl2;
+        }
+        tl = tl2;
+        const int snc = ncoef_of(t, t.level[r.i2o_src[pf]]);
+        const T *B = B0 + key;  // the run's stored block
+        __syncthreads();  // the previous run's stores have read its pair table
+        for (int j = threadIdx.x; j < GT_NB * TG_Q; j += blockDim.x) {
+            const int b = j / TG_Q, jj = j % TG_Q;
+            if (b < nb && jj < bn[b]) {
+                const int e = bs[b] + jj;
+                const int p = gt.pair[e];
+                run_src[j] = r.pair_src[p] * nrhs;
+                run_perm[j] = r.pair_perm ? r.pair_perm[p] : -1;
+                run_slot[j] = gt.slot[e];
+            }
+        }
+        for (int m0 = 0; m0 < nc; m0 += TG_M) {
+            const int mt = min(TG_M, nc - m0);
+            MmaAcc<A> acc[GT_NB];
+#pragma unroll
+            for (int b = 0; b < GT_NB; ++b) acc[b].zero();
+            for (int k0 = 0; k0 < snc; k0 += TG_K) {
+                const int kc = min(TG_K, snc - k0);
+                __syncthreads();
+                // the block's 64 x 32 piece: forward reads the stored (r, t) block nc x snc along
+                // its rows, transposed orientations the stored (t, r) block snc x nc along k
+                if (fwd) {
+                    for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
+                        const int i = idx % mt, k = idx / mt;
+                        Ms[i * TG_LD + k] = k < kc ? wide(cj(B[m0 + i + (int64_t)(k0 + k) * nc], adj)) : A{};
+                    }
+                } else {
+                    for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
+                        const int k = idx % TG_K, i = idx / TG_K;
+                        Ms[i * TG_LD + k] = k < kc ? wide(cj(B[k0 + k + (int64_t)(m0 + i) * snc], adj)) : A{};
+                    }
+                }
+                // each block's moments: column c = pair c / nq, right-hand side c % nq, read
+                // through the pair's column permutation (forward) or row permutation (transposed)
+                for (int b = 0; b < nb; ++b) {
+                    const int ncol = bn[b] * nq;
+                    A *xs = Xs + b * TG_K * TG_Q;
+                    for (int idx = threadIdx.x; idx < TG_K * ncol; idx += blockDim.x) {
+                        const int k = idx % TG_K, c = idx / TG_K;
+                        A v{};
+                        if (k < kc) {
+                            const int j = b * TG_Q + c / nq;
+                            const int64_t ps = run_perm[j];
+                            const int kk = ps < 0 ? k0 + k : m.perm[ps + (fwd ? 2 * snc : 0) + k0 + k];
+                            v = wide(am[run_src[j] + (int64_t)(c % nq) * snc + kk]);
+                        }
+                        xs[k * TG_Q + c] = v;
+                    }
+                }
+                __syncthreads();
+                if (8 * warp < mt) {
+                    const A *mrow = Ms + (8 * warp + g4) * TG_LD + t4;
+#pragma unroll
+                    for (int k = 0; k < TG_K; k += 4) {
+                        const A a = mrow[k];
+#pragma unroll
+                        for (int b = 0; b < GT_NB; ++b) {
+                            if (b < nb) {
+                                const A *xcol = Xs + b * TG_K * TG_Q + (t4 + k) * TG_Q + g4;
+                                const A bb[2] = {xcol[0], xcol[8]};
+                                acc[b].step(a, bb);
+                            }
+                        }
+                    }
+                }
+            }
+            // the blocks' products into the receivers' sums, one block after another
+#pragma unroll
+            for (int b = 0; b < GT_NB; ++b) {
+                if (b < nb) {
+                    __syncthreads();
+                    mma_store(acc[b], mt, bn[b] * nq, [&](int i, int c, A v) {
+                        const int j = b * TG_Q + c / nq;
+                        const int64_t ps = run_perm[j];
+                        const int row = ps < 0 ? m0 + i : m.perm[ps + (fwd ? 0 : 2 * nc) + m0 + i];
+                        A &sum = Sum[(run_slot[j] * nq + c % nq) * nc + row];
+                        sum = sum + v;
+                    });
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < nr * nq * nc; o += blockDim.x) {
+        const int ls = o / (nq * nc);
+        narrow(Sum[o], dm[r.mom_off[gt.rcv[r0 + ls]] * nrhs + o % (nq * nc)]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // B2 by sibling groups: the Toeplitz I2O of the receiving children of one parent together. One CTA
 // per (group, block of right-hand sides), one thread per stored frequency. The CTA walks the union
 // of the siblings' sources once; each source spectrum value is loaded once and applied from
@@ -1622,6 +1769,31 @@ cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DS
         }
         err = cube7 ? launch(toeplitz_in_kernel<T, 7, 7>)
                     : (maxaxis <= 7 ? launch(toeplitz_in_kernel<T, 7, 0>) : launch(toeplitz_in_kernel<T, 15, 0>));
+    });
+    return err != cudaSuccess ? err : cudaGetLastError();
+}
+
+bool i2o_grouped_eligible(bool cplx, const DMap &m, int nq, int maxcoef) {
+    if (m.coupling_kind != H2B_COUPLING_DENSE || (cplx ? 2 : 1) * nq > GT_MAX_COLS) return false;
+    // the staged piece, the column blocks and the chunk's sums (FP64) fit in a CTA's shared memory
+    const size_t a = cplx ? sizeof(cdouble) : sizeof(double);
+    const size_t nb = cplx ? gt_nb<cdouble>() : gt_nb<double>();
+    return (TG_M * TG_LD + nb * TG_K * TG_Q + (size_t)GT_R * nq * maxcoef) * a <= 227u * 1024u - 4096u;
+}
+
+cudaError_t launch_i2o_grouped(bool cplx, int precision, const DMap &m, const DSide &recv, const DSide &src,
+                               const GroupTiles &gt, int maxcoef, const FarArgs &fa, cudaStream_t st) {
+    if (gt.nchunks == 0) return cudaSuccess;
+    const int nq = m.ncomp * fa.nrhs;
+    cudaError_t err = cudaSuccess;
+    H2B_DISPATCH_T(cplx, precision, {
+        using A = typename ScalarTraits<T>::Acc;
+        const size_t sm = (size_t)(TG_M * TG_LD + gt_nb<A>() * TG_K * TG_Q + GT_R * nq * maxcoef) * sizeof(A);
+        auto kern = &i2o_grouped_kernel<T>;
+        err = allow_smem(kern, sm);
+        if (err == cudaSuccess)
+            kern<<<gt.nchunks, 256, sm, st>>>(m, recv, src, gt, fa.mode, fa.nrhs, static_cast<const T *>(fa.am),
+                                              static_cast<T *>(fa.dm));
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
