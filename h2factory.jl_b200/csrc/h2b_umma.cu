@@ -7,30 +7,34 @@
 // concatenated pairs: D[nc x nq] = [op(B_1) op(B_2) ...] [m_1; m_2; ...].
 //
 // One CTA per (receiver, 128-row tile of its coefficients, tile of right-hand sides), one CTA per
-// SM, warp-specialised; the K dimension streams in chunks of 16 FP32 values through UM_NS stages,
+// SM, warp-specialised; the K dimension streams in chunks of 32 FP32 values through UM_NS stages,
 // and every hand-off is an mbarrier (no block barrier inside the loop):
-//   * coupling warps (0-3), one thread per tile row: load the row's 16 values of chunk c + 3 into
-//     a register ring (the couplings are L2-resident; every load reads a valid clamped address and
-//     the values past the block are zeroed at split time, so nothing waits on a load early), split
-//     chunk c into TF32 high parts and rounded remainders and write them into a tensor-memory
-//     stage with tcgen05.st. The MMAs take this operand (A) straight from tensor memory;
-//   * moment warps (4-6): cp.async each chunk's source moments into a raw shared-memory ring (the
-//     permuted source rows of a symmetry-reduced pair are fetched a chunk ahead), then write them
-//     as the B operand, TF32 high parts plus remainders, in the canonical no-swizzle K-major layout;
+//   * coupling warps (0-3), one thread per tile row: each warp bulk-copies (cp.async.bulk) a
+//     quarter of the stored columns that chunk c + 3 reads (column kmap[k] of the pair's block:
+//     the column permutation of a symmetry-reduced pair is which column is fetched) into a
+//     shared-memory ring; every thread then reads its row of the chunk (rowmap applied by the row
+//     it reads), splits the 32 values into TF32 high parts and rounded remainders and writes them
+//     into a tensor-memory stage with tcgen05.st. The MMAs take this operand (A) straight from
+//     tensor memory. Couplings without whole 16-byte columns are read row by row from global
+//     memory into a register ring instead;
+//   * moment warps (4-6): cp.async each chunk's source moments into a raw shared-memory ring four
+//     chunks ahead, then write them as the B operand, TF32 high parts plus remainders, in the
+//     canonical no-swizzle K-major layout (a complex piece is split once for its two rows);
 //   * one MMA thread (warp 11): per 8-wide k step the products hi*hi + hi*lo + lo*hi (the lo*lo
 //     term is below FP32 rounding), N = 64 columns each, into an FP32 accumulator in tensor memory;
 //     one commit per chunk releases both operand stages. A tcgen05.mma costs its issuing thread
 //     about 50 cycles whatever its N (measured), so products are made as wide as the block allows;
 //   * drain warps (7-10, one per tensor-memory lane quarter): the tensor cores round each
 //     accumulation toward zero, so one FP32 accumulator over a whole interaction list loses ~1e-4;
-//     accumulators live for 8 chunks only, two alternate, and each finished one is added into an
-//     FP64 sum in tensor memory, which the epilogue rounds once into the FP32 moments.
+//     accumulators live for 64 values of K (2 chunks) only, two alternate, and each finished one is
+//     added into an FP64 sum in tensor memory, which the epilogue rounds once into the FP32 moments.
 //
 // Complex maps run as real GEMMs: with B = Br + i Bi and m = mr + i mi,
 //   [Re l | Im l] = [Br Bi] (interleaved along k) x [[mr, mi]; [-mi, mr]] (interleaved rows),
 // so the coupling's interleaved (re, im) storage is the A operand as it lies in memory and each
 // moment value feeds two B rows (Re rows (mr, -mi), Im rows (mi, mr)). Adjoint maps conjugate B;
-// symmetry-reduced couplings apply their row / column permutations in the load addresses.
+// symmetry-reduced couplings apply their row / column permutations in which rows and columns are
+// read. FP32 dense couplings are also stored transposed, so every orientation copies columns.
 //
 // Every wait on an mbarrier is bounded: a wait that gives up counts itself in a device counter
 // (h2b_tensor_wait_timeouts) and sets the CTA's abort flag; every role then leaves its loop, the
