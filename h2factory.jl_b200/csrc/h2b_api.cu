@@ -483,8 +483,9 @@ h2b_status upload_list(h2b_core *c, const std::vector<int> &v, int **dst) {
 
 // Chunks and tiles of the grouped dense I2O (GroupTiles) for the receiving nodes of side `s`:
 // chunks of up to GT_R consecutive receiving nodes of one level -- fewer when the map has too few
-// receiving nodes to give two chunks per SM with full chunks (down to 4 per chunk: a small map
-// trades block reuse for SMs); per chunk, its pairs sorted by
+// receiving nodes to give every SM a full chunk (down to 4 per chunk: a small map trades block
+// reuse for SMs; with two chunks per SM as the target the large maps lost more reuse than they
+// gained SMs); per chunk, its pairs sorted by
 // stored block, then by their rank among the receiver's pairs reading that block, then by receiver,
 // and cut into tiles of at most GT_P pairs with one block and distinct receivers.
 h2b_status build_group_tiles(h2b_core *c, const h2b_side_desc &s, SideHost &h,
@@ -495,7 +496,7 @@ h2b_status build_group_tiles(h2b_core *c, const h2b_side_desc &s, SideHost &h,
     if (recv.empty()) return H2B_OK;
     int nsm = 148;
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-    const int R = std::min(GT_R, std::max(4, (int)(recv.size() / (2 * (size_t)nsm))));
+    const int R = std::min(GT_R, std::max(4, (int)(recv.size() / (size_t)nsm)));
     std::vector<int> chunk_ptr{0}, rcv, tile_ptr{0}, tile_pp{0}, pair;
     std::vector<unsigned char> slot;
     struct E { int64_t key; int rank, slot, p; };
