@@ -1316,7 +1316,7 @@ h2b_status run_i2o(h2b_core *c, const SideHost &D, const SideHost &A, const FarA
         return H2B_OK;
     }
     const bool cplx = c->field == H2B_COMPLEX;
-    if (D.grp.nchunks > 0 && i2o_grouped_eligible(cplx, c->dmap, c->dmap.ncomp * fa.nrhs, maxcoef)) {
+    if (D.grp.nchunks > 0 && i2o_grouped_eligible(cplx, c->precision, c->dmap, c->dmap.ncomp * fa.nrhs, maxcoef)) {
         CUDA_TRY(launch_i2o_grouped(cplx, c->precision, c->dmap, D.d, A.d, D.grp, maxcoef, fa, st));
         return H2B_OK;
     }

@@ -221,7 +221,7 @@ cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const D
 // 13 / 26 / 65 / 73 ms for 1-4 real right-hand sides against 98 / 150 / 152 ms for the per-node
 // tile kernel and 84 ms for the tcgen05 kernel from 4 columns on).
 constexpr int GT_MAX_COLS = 4;
-bool i2o_grouped_eligible(bool cplx, const DMap &m, int nq, int maxcoef);
+bool i2o_grouped_eligible(bool cplx, int precision, const DMap &m, int nq, int maxcoef);
 cudaError_t launch_i2o_grouped(bool cplx, int precision, const DMap &m, const DSide &recv, const DSide &src,
                                const GroupTiles &gt, int maxcoef, const FarArgs &fa, cudaStream_t st);
 cudaError_t launch_transfer_down(bool cplx, int precision, const DMap &m, const DSide &s,

@@ -1139,8 +1139,9 @@ __global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, cons
 
 // ---------------------------------------------------------------------------------------------
 // B1 for few right-hand sides, grouped by stored block (GroupTiles). One CTA per chunk of receiving
-// nodes of one level. For each tile (pairs reading one stored block, distinct receivers) the block
-// is staged in 64 x 32 pieces once for up to TG_Q columns (pairs x right-hand sides) and applied
+// nodes of one level. For each run of pairs reading one stored block the block is staged in 64 x 32
+// pieces (cp.async, two stages: the next chunk's copies fly while the tensor cores work on this
+// one), each piece applied to up to GT_NB column blocks of TG_Q columns (pairs x right-hand sides)
 // on the FP64 tensor cores; each pair's symmetry permutation moves into the gather of its moments
 // (column permutation) and the row its products land on (row permutation), the canonical form of
 // symmetryreduceddense.jl:84-95. Products add into the chunk's sums in shared memory; the tiles
@@ -1152,14 +1153,29 @@ __global__ void __launch_bounds__(512) i2o_kernel(DMap m, DSide r, DSide t, cons
 // 4 doubles per block and lane for real sums, 8 for complex)
 template <class A> constexpr int gt_nb() { return sizeof(A) == 16 ? 4 : 8; }
 
+// element copy global -> shared (cp.async); ok = false writes zeros and reads nothing
+template <int EB>
+__device__ __forceinline__ void cp_async_elem(void *dst, const void *src, bool ok) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "n"(EB), "r"(ok ? EB : 0)
+                 : "memory");
+}
+
 template <class T>
 __global__ void __launch_bounds__(256)
-i2o_grouped_kernel(DMap m, DSide r, DSide t, GroupTiles gt, int mode, int nrhs, const T *__restrict__ am,
-                   T *__restrict__ dm) {
+i2o_grouped_kernel(DMap m, DSide r, DSide t, GroupTiles gt, int mode, int nrhs, int maxcoef,
+                   const T *__restrict__ am, T *__restrict__ dm) {
     using A = typename ScalarTraits<T>::Acc;
     constexpr int GT_NB = gt_nb<A>();
+    constexpr int EB = sizeof(T);
+    constexpr int MS = TG_M * TG_LD, XS = GT_NB * TG_K * TG_Q;  // one stage of the block / moments
     extern __shared__ unsigned char smem_raw[];
-    A *Ms = reinterpret_cast<A *>(smem_raw), *Xs = Ms + TG_M * TG_LD, *Sum = Xs + GT_NB * TG_K * TG_Q;
+    // the receivers' FP64 sums, then two stages of the block piece and the moments in the storage
+    // type (copied with cp.async one chunk ahead, widened when the products read them)
+    const int nq = m.ncomp * nrhs;
+    A *Sum = reinterpret_cast<A *>(smem_raw);
+    T *Mst = reinterpret_cast<T *>(Sum + GT_R * nq * maxcoef);
+    T *Xst = Mst + 2 * MS;
     // per pair of the current run (slot b * TG_Q + j: pair j of column block b): its moments' offset,
     // its permutation set (-1: none) and its receiver's position in the chunk
     __shared__ int64_t run_src[GT_NB * TG_Q], run_perm[GT_NB * TG_Q];
@@ -1167,7 +1183,6 @@ i2o_grouped_kernel(DMap m, DSide r, DSide t, GroupTiles gt, int mode, int nrhs, 
     const int ch = blockIdx.x;
     const int r0 = gt.chunk_ptr[ch], nr = gt.chunk_ptr[ch + 1] - r0;
     const int nc = ncoef_of(r, r.level[gt.rcv[r0]]);
-    const int nq = m.ncomp * nrhs;
     const bool fwd = mode == H2B_FORWARD, adj = mode == H2B_ADJOINT;
     const T *B0 = static_cast<const T *>(m.cpl);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g4 = lane >> 2, t4 = lane & 3;
@@ -1206,60 +1221,71 @@ i2o_grouped_kernel(DMap m, DSide r, DSide t, GroupTiles gt, int mode, int nrhs, 
                 run_slot[j] = gt.slot[e];
             }
         }
+        __syncthreads();
+        const int nk = (snc + TG_K - 1) / TG_K;
         for (int m0 = 0; m0 < nc; m0 += TG_M) {
             const int mt = min(TG_M, nc - m0);
-            MmaAcc<A> acc[GT_NB];
-#pragma unroll
-            for (int b = 0; b < GT_NB; ++b) acc[b].zero();
-            for (int k0 = 0; k0 < snc; k0 += TG_K) {
-                const int kc = min(TG_K, snc - k0);
-                __syncthreads();
-                // the block's 64 x 32 piece: forward reads the stored (r, t) block nc x snc along
-                // its rows, transposed orientations the stored (t, r) block snc x nc along k
+            // chunk kc's copies into stage kc & 1: the block piece (forward reads the stored (r, t)
+            // block nc x snc down its columns, transposed orientations the stored (t, r) block
+            // snc x nc along k) and each column block's moments, read through the pair's column
+            // permutation (forward) or row permutation (transposed); past the block: zeros
+            auto issue = [&](int kc) {
+                const int k0 = kc * TG_K, kv = min(TG_K, snc - k0);
+                T *ms = Mst + (kc & 1) * MS;
                 if (fwd) {
                     for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
                         const int i = idx % mt, k = idx / mt;
-                        Ms[i * TG_LD + k] = k < kc ? wide(cj(B[m0 + i + (int64_t)(k0 + k) * nc], adj)) : A{};
+                        const bool ok = k < kv;
+                        cp_async_elem<EB>(ms + i * TG_LD + k, ok ? B + m0 + i + (int64_t)(k0 + k) * nc : B, ok);
                     }
                 } else {
                     for (int idx = threadIdx.x; idx < mt * TG_K; idx += blockDim.x) {
                         const int k = idx % TG_K, i = idx / TG_K;
-                        Ms[i * TG_LD + k] = k < kc ? wide(cj(B[k0 + k + (int64_t)(m0 + i) * snc], adj)) : A{};
+                        const bool ok = k < kv;
+                        cp_async_elem<EB>(ms + i * TG_LD + k, ok ? B + k0 + k + (int64_t)(m0 + i) * snc : B, ok);
                     }
                 }
-                // each block's moments: column c = pair c / nq, right-hand side c % nq, read
-                // through the pair's column permutation (forward) or row permutation (transposed)
+                T *xst = Xst + (kc & 1) * XS;
                 for (int b = 0; b < nb; ++b) {
                     const int ncol = bn[b] * nq;
-                    A *xs = Xs + b * TG_K * TG_Q;
+                    T *xs = xst + b * TG_K * TG_Q;
                     for (int idx = threadIdx.x; idx < TG_K * ncol; idx += blockDim.x) {
                         const int k = idx % TG_K, c = idx / TG_K;
-                        A v{};
-                        if (k < kc) {
-                            const int j = b * TG_Q + c / nq;
-                            const int64_t ps = run_perm[j];
-                            const int kk = ps < 0 ? k0 + k : m.perm[ps + (fwd ? 2 * snc : 0) + k0 + k];
-                            v = wide(am[run_src[j] + (int64_t)(c % nq) * snc + kk]);
-                        }
-                        xs[k * TG_Q + c] = v;
+                        const int j = b * TG_Q + c / nq;
+                        const bool ok = k < kv;
+                        const int64_t ps = run_perm[j];
+                        const int kk = !ok ? 0 : (ps < 0 ? k0 + k : m.perm[ps + (fwd ? 2 * snc : 0) + k0 + k]);
+                        cp_async_elem<EB>(xs + k * TG_Q + c, am + run_src[j] + (int64_t)(c % nq) * snc + kk, ok);
                     }
                 }
-                __syncthreads();
+            };
+            MmaAcc<A> acc[GT_NB];
+#pragma unroll
+            for (int b = 0; b < GT_NB; ++b) acc[b].zero();
+            issue(0);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            for (int kc = 0; kc < nk; ++kc) {
+                if (kc + 1 < nk) issue(kc + 1);  // its stage was last read before the barrier below
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                asm volatile("cp.async.wait_group 1;" ::: "memory");  // this thread's chunk kc
+                __syncthreads();                                      // ... and everyone's
                 if (8 * warp < mt) {
-                    const A *mrow = Ms + (8 * warp + g4) * TG_LD + t4;
+                    const T *mrow = Mst + (kc & 1) * MS + (8 * warp + g4) * TG_LD + t4;
+                    const T *xst = Xst + (kc & 1) * XS;
 #pragma unroll
                     for (int k = 0; k < TG_K; k += 4) {
-                        const A a = mrow[k];
+                        const A a = wide(cj(mrow[k], adj));
 #pragma unroll
                         for (int b = 0; b < GT_NB; ++b) {
                             if (b < nb) {
-                                const A *xcol = Xs + b * TG_K * TG_Q + (t4 + k) * TG_Q + g4;
-                                const A bb[2] = {xcol[0], xcol[8]};
+                                const T *xcol = xst + b * TG_K * TG_Q + (t4 + k) * TG_Q + g4;
+                                const A bb[2] = {wide(xcol[0]), wide(xcol[8])};
                                 acc[b].step(a, bb);
                             }
                         }
                     }
                 }
+                __syncthreads();  // stage kc & 1 is free for chunk kc + 2
             }
             // the blocks' products into the receivers' sums, one block after another
 #pragma unroll
@@ -1773,12 +1799,14 @@ cudaError_t launch_toeplitz_in(bool cplx, int precision, const DMap &m, const DS
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 
-bool i2o_grouped_eligible(bool cplx, const DMap &m, int nq, int maxcoef) {
+bool i2o_grouped_eligible(bool cplx, int precision, const DMap &m, int nq, int maxcoef) {
     if (m.coupling_kind != H2B_COUPLING_DENSE || (cplx ? 2 : 1) * nq > GT_MAX_COLS) return false;
-    // the staged piece, the column blocks and the chunk's sums (FP64) fit in a CTA's shared memory
+    // the chunk's sums (FP64) and two stages of the block piece and the moments (storage type)
+    // fit in a CTA's shared memory
     const size_t a = cplx ? sizeof(cdouble) : sizeof(double);
+    const size_t e = (cplx ? 2 : 1) * (precision == H2B_FP32 ? 4 : 8);
     const size_t nb = cplx ? gt_nb<cdouble>() : gt_nb<double>();
-    return (TG_M * TG_LD + nb * TG_K * TG_Q + (size_t)GT_R * nq * maxcoef) * a <= 227u * 1024u - 4096u;
+    return 2 * (TG_M * TG_LD + nb * TG_K * TG_Q) * e + (size_t)GT_R * nq * maxcoef * a <= 227u * 1024u - 4096u;
 }
 
 cudaError_t launch_i2o_grouped(bool cplx, int precision, const DMap &m, const DSide &recv, const DSide &src,
@@ -1788,12 +1816,13 @@ cudaError_t launch_i2o_grouped(bool cplx, int precision, const DMap &m, const DS
     cudaError_t err = cudaSuccess;
     H2B_DISPATCH_T(cplx, precision, {
         using A = typename ScalarTraits<T>::Acc;
-        const size_t sm = (size_t)(TG_M * TG_LD + gt_nb<A>() * TG_K * TG_Q + GT_R * nq * maxcoef) * sizeof(A);
+        const size_t sm = (size_t)GT_R * nq * maxcoef * sizeof(A) +
+                          2 * (size_t)(TG_M * TG_LD + gt_nb<A>() * TG_K * TG_Q) * sizeof(T);
         auto kern = &i2o_grouped_kernel<T>;
         err = allow_smem(kern, sm);
         if (err == cudaSuccess)
-            kern<<<gt.nchunks, 256, sm, st>>>(m, recv, src, gt, fa.mode, fa.nrhs, static_cast<const T *>(fa.am),
-                                              static_cast<T *>(fa.dm));
+            kern<<<gt.nchunks, 256, sm, st>>>(m, recv, src, gt, fa.mode, fa.nrhs, maxcoef,
+                                              static_cast<const T *>(fa.am), static_cast<T *>(fa.dm));
     });
     return err != cudaSuccess ? err : cudaGetLastError();
 }
