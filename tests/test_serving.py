@@ -261,3 +261,36 @@ def test_inflight_cap_coalesces_and_serves_oldest_first():
     assert np.mean(srv.blocks) > 3  # requests waited behind the single block and coalesced
     # round robin by age: no map waits for two launches of another while it has a request queued
     assert all(ex.order[k] != ex.order[k + 1] for k in range(min(6, len(ex.order) - 1)))
+
+
+def test_open_loop_window_accounting(monkeypatch):
+    """The serving benchmark's open-loop window (bench.py) against the CPU executor: arrivals follow
+    the Poisson schedule, requests not started when the window closes are cancelled and dropped,
+    every other request completes, and latency counts from the scheduled arrival."""
+    import os
+    import sys
+
+    import torch
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    import bench
+
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    rng = np.random.default_rng(12)
+    maps = mats(rng, [24, 24], cplx=False)
+    srv = MatvecServer(DenseExecutor(delay=0.004), budget_bytes=1e9, max_block=8, slots=1, max_inflight=1)
+    for i, M in enumerate(maps):
+        srv.add_map(i, M)
+    xs = {(i, w): (rng.standard_normal(24) if w == 1 else rng.standard_normal((24, w))) for i in range(2) for w in (1, 4)}
+    light = bench._open_loop(srv, xs, 2, 1, 200.0, 0.3, rng)      # well under capacity
+    heavy = bench._open_loop(srv, xs, 2, 4, 20000.0, 0.3, rng)    # far over it
+    srv.close()
+    for r in (light, heavy):
+        assert r["completed"] + r["cancelled"] == r["requests"]
+        assert r["completed_in_window"] <= r["completed"]
+        assert r["achieved_rhs_per_s"] == pytest.approx(r["achieved_req_per_s"] * r["rhs_per_request"])
+    assert light["cancelled"] <= 2 and light["p99_ms"] < 100
+    assert heavy["cancelled"] > 0 and heavy["mean_block_rhs"] > 4  # queued requests coalesced
+    assert heavy["achieved_req_per_s"] < 20000.0
