@@ -217,9 +217,10 @@ cudaError_t set_umma_wait_limit(unsigned limit);
 cudaError_t launch_i2o_siblings(bool cplx, int precision, const DMap &m, const DSide &recv,
                                 const SibGroups &g, int maxslen, const FarArgs &fa, cudaStream_t st);
 // The grouped dense I2O (GroupTiles) for W x nq <= GT_MAX_COLS field columns (W = 2 complex);
-// wider blocks take the tensor-core I2O (measured on a 65,536-point Laplace map, p = 6: grouped
-// 13 / 26 / 65 / 73 ms for 1-4 real right-hand sides against 98 / 150 / 152 ms for the per-node
-// tile kernel and 84 ms for the tcgen05 kernel from 4 columns on).
+// wider blocks take the tensor-core I2O (measured on a 65,536-point Laplace map, p = 6, FP32 form:
+// grouped 8.5 / 16.8 / 41.5 / 46.6 / 74.6 / 96.2 ms for 1-6 real right-hand sides against
+// 98 / 150 / 152 ms for the per-node tile kernel and 84 ms for the tcgen05 kernel from 4 columns
+// on; with 5 and 6 columns grouped, the batched-uneven pass did not change).
 constexpr int GT_MAX_COLS = 4;
 bool i2o_grouped_eligible(bool cplx, int precision, const DMap &m, int nq, int maxcoef);
 cudaError_t launch_i2o_grouped(bool cplx, int precision, const DMap &m, const DSide &recv, const DSide &src,
